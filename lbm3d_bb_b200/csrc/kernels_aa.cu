@@ -1,0 +1,565 @@
+// kernels_aa.cu — configurable D3Q19 step as one fused AA-pattern kernel.
+//
+// One population array A (SoA: A[d*plane + node]) is updated in place.  Steps
+// alternate between two phases:
+//   even phase: node x reads S[d,x] = A[d][x], collides, and writes its
+//               post-collision f*[dbar] into A[d][x] (swapped slots);
+//   odd phase:  node x pulls S[d,x] = A[dbar][x - c_d], collides, and pushes
+//               f*[d] into A[d][x + c_d].
+// Every slot is read and written by exactly one thread per phase, so the kernel
+// is race-free and moves 2 * 19 populations per node per step.
+//
+// Boundaries are "own-slot" rules: when the source x - c_d of an incoming
+// population lies outside a non-periodic face or in a solid node, the value is a
+// function of node x alone (bounce-back, equilibrium, zero-gradient) and is kept
+// in A[d][x], a slot no other node touches in either phase.  This covers
+// SolidBC.jl's moving-wall bounce-back (SBB!_gpu, SolidBC.jl:160-210) and the
+// face conditions of OtherBC.jl (velocity_BC!_gpu, OtherBC.jl:112-169) in the
+// configurable form.  Links are resolved from the node flag bytes (no CSR on the
+// hot path); the momentum exchange of MEA.jl:76-116 is accumulated in FP64 and
+// reduced with warp shuffles, one atomic per block and component.
+//
+// Moving bodies: the flags of the previous step decide which incoming slots hold
+// boundary values (read side), the current flags decide what is written; nodes
+// uncovered by the body are refilled with the equilibrium at the body velocity.
+// A fresh node's emitted populations toward old fluid neighbours are recomputed by
+// those neighbours (same __noinline__ routine, bit-identical), which keeps the odd
+// phase race-free.
+#include "lbm_internal.cuh"
+#include "lbm_kernels.h"
+
+namespace lbm {
+
+// ---- storage policies ------------------------------------------------------------
+struct StF32 {
+  using S = float;
+  using C = float;
+  static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
+  static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
+};
+struct StF64 {
+  using S = double;
+  using C = double;
+  static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
+  static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
+};
+// FP16 deviation from the rest equilibrium: stored h = f - w_d*rho0, computed in FP32.
+struct StF16 {
+  using S = __half;
+  using C = float;
+  static __device__ __forceinline__ C ld(const S* p, int d, C rho0) {
+    return wgt<float>(d) * rho0 + __half2float(*p);
+  }
+  static __device__ __forceinline__ void st(S* p, C v, int d, C rho0) {
+    *p = __float2half_rn(v - wgt<float>(d) * rho0);
+  }
+};
+
+// ---- collision ---------------------------------------------------------------------
+template <class C>
+struct Coll {
+  C om_p, om_m;  // relaxation rates
+  C gx, gy, gz;  // body acceleration
+};
+
+// Moments of f: rho, j, then u = j/rho + g/2 (Guo).  Sums run in direction
+// order with the zero terms of c_d skipped.
+template <class C, bool FORCE>
+__device__ __forceinline__ void moments(const C* f, const Coll<C>& k, C& rho, C& ux, C& uy, C& uz) {
+  C r = f[0], jx = C(0), jy = C(0), jz = C(0);
+#pragma unroll
+  for (int d = 1; d < Q; d++) r += f[d];
+#pragma unroll
+  for (int d = 0; d < Q; d++) {
+    if (cx(d) == 1) jx += f[d];
+    if (cx(d) == -1) jx -= f[d];
+    if (cy(d) == 1) jy += f[d];
+    if (cy(d) == -1) jy -= f[d];
+    if (cz(d) == 1) jz += f[d];
+    if (cz(d) == -1) jz -= f[d];
+  }
+  C inv = C(1) / r;
+  rho = r;
+  ux = jx * inv;
+  uy = jy * inv;
+  uz = jz * inv;
+  if (FORCE) {
+    ux += C(0.5) * k.gx;
+    uy += C(0.5) * k.gy;
+    uz += C(0.5) * k.gz;
+  }
+}
+
+template <class C>
+__device__ __forceinline__ C cdot(int d, C ux, C uy, C uz) {
+  C s = C(0);
+  if (cx(d) == 1) s += ux;
+  if (cx(d) == -1) s -= ux;
+  if (cy(d) == 1) s += uy;
+  if (cy(d) == -1) s -= uy;
+  if (cz(d) == 1) s += uz;
+  if (cz(d) == -1) s -= uz;
+  return s;
+}
+
+template <class C>
+__device__ __forceinline__ C feq(int d, C rho, C ux, C uy, C uz) {
+  C cu = cdot<C>(d, ux, uy, uz);
+  C usq = ux * ux + uy * uy + uz * uz;
+  return wgt<C>(d) * rho * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * usq);
+}
+
+// BGK / TRT with Guo forcing; f -> p (post-collision).
+template <class C, bool TRT, bool FORCE>
+__device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rho, C ux, C uy, C uz) {
+  const C usq = ux * ux + uy * uy + uz * uz;
+  const C base = C(1) - C(1.5) * usq;
+  C Fx = C(0), Fy = C(0), Fz = C(0), uF = C(0);
+  if (FORCE) {
+    Fx = rho * k.gx;
+    Fy = rho * k.gy;
+    Fz = rho * k.gz;
+    uF = ux * Fx + uy * Fy + uz * Fz;
+  }
+  if (!TRT) {
+    const C fac = C(1) - C(0.5) * k.om_p;
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      const C wr = wgt<C>(d) * rho;
+      const C cu = cdot<C>(d, ux, uy, uz);
+      const C fe = wr * (base + cu * (C(3) + C(4.5) * cu));
+      C v = f[d] - k.om_p * (f[d] - fe);
+      if (FORCE) {
+        const C cF = cdot<C>(d, Fx, Fy, Fz);
+        v += fac * wgt<C>(d) * (C(3) * (cF - uF) + C(9) * cu * cF);
+      }
+      p[d] = v;
+    }
+  } else {
+    const C fac_p = C(1) - C(0.5) * k.om_p, fac_m = C(1) - C(0.5) * k.om_m;
+#pragma unroll
+    for (int d = 0; d < 18; d += 2) {
+      const int o = d + 1;
+      const C wr = wgt<C>(d) * rho;
+      const C cu = cdot<C>(d, ux, uy, uz);
+      const C ep = wr * (base + C(4.5) * cu * cu);
+      const C em = wr * (C(3) * cu);
+      const C fp = C(0.5) * (f[d] + f[o]);
+      const C fm = C(0.5) * (f[d] - f[o]);
+      C rp = k.om_p * (fp - ep);
+      C rm = k.om_m * (fm - em);
+      C a = f[d] - rp - rm;
+      C b = f[o] - rp + rm;
+      if (FORCE) {
+        const C cF = cdot<C>(d, Fx, Fy, Fz);
+        const C sp = wgt<C>(d) * (C(9) * cu * cF - C(3) * uF);
+        const C sm = wgt<C>(d) * (C(3) * cF);
+        a += fac_p * sp + fac_m * sm;
+        b += fac_p * sp - fac_m * sm;
+      }
+      p[d] = a;
+      p[o] = b;
+    }
+    {
+      const C wr = wgt<C>(18) * rho;
+      const C ep = wr * base;
+      C v = f[18] - k.om_p * (f[18] - ep);
+      if (FORCE) v += fac_p * wgt<C>(18) * (C(-3) * uF);
+      p[18] = v;
+    }
+  }
+}
+
+// Wall velocity of the moving body at lattice point (px,py,pz).
+__device__ __forceinline__ void wall_velocity(const Kinematics& k, double px, double py, double pz,
+                                              double& wx, double& wy, double& wz) {
+  const double rx = px - k.center[0], ry = py - k.center[1], rz = pz - k.center[2];
+  wx = k.vel[0] + (k.omega[1] * rz - k.omega[2] * ry);
+  wy = k.vel[1] + (k.omega[2] * rx - k.omega[0] * rz);
+  wz = k.vel[2] + (k.omega[0] * ry - k.omega[1] * rx);
+}
+
+// Post-collision state of a node refilled with feq(rho0, u_wall(node)).  Not
+// inlined: a fresh node and each of its old-fluid neighbours call the same code
+// and therefore obtain bit-identical values.
+template <class C, bool TRT, bool FORCE>
+__device__ __noinline__ void fresh_state(Coll<C> k, Kinematics kin, C rho0, int x, int y, int z,
+                                         C* p, C* mom) {
+  double wx, wy, wz;
+  wall_velocity(kin, x + 0.5, y + 0.5, z + 0.5, wx, wy, wz);
+  C f[Q];
+#pragma unroll
+  for (int d = 0; d < Q; d++) f[d] = feq<C>(d, rho0, C(wx), C(wy), C(wz));
+  C rho, ux, uy, uz;
+  moments<C, FORCE>(f, k, rho, ux, uy, uz);
+  collide<C, TRT, FORCE>(f, p, k, rho, ux, uy, uz);
+  mom[0] = rho;
+  mom[1] = ux;
+  mom[2] = uy;
+  mom[3] = uz;
+}
+
+// ---- the step kernel ------------------------------------------------------------------
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__global__ void __launch_bounds__(256) aa_step_kernel(const __grid_constant__ AAParams p, typename SP::S* __restrict__ A,
+                                                      const uint8_t* __restrict__ flags) {
+  using S = typename SP::S;
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = (x < g.nx) && (y < g.ny);
+  const long long i = inb ? node_index(g, x, y, z) : 0;
+  const uint8_t fl = inb ? flags[i] : (uint8_t)F_SOLID;
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  const C rho0 = C(p.rho0);
+  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
+
+  if (p.zero_next && x == 0 && y == 0 && z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    // clear the force slot of the next step (read by the next launch only)
+#pragma unroll
+    for (int c = 0; c < 6; c++) p.zero_next[c] = 0.0;
+  }
+
+  if (!(fl & F_SOLID)) {
+    const long long nxl = g.nx, nxy = (long long)g.nx * g.ny;
+    // neighbour coordinates; -1 when outside a non-periodic axis
+    const int xs0 = x == 0 ? (g.per[0] ? g.nx - 1 : -1) : x - 1;
+    const int xs2 = x == g.nx - 1 ? (g.per[0] ? 0 : -1) : x + 1;
+    const int ys0 = y == 0 ? (g.per[1] ? g.ny - 1 : -1) : y - 1;
+    const int ys2 = y == g.ny - 1 ? (g.per[1] ? 0 : -1) : y + 1;
+    const int zs0 = z == 0 ? (g.per[2] ? g.nz - 1 : -1) : z - 1;
+    const int zs2 = z == g.nz - 1 ? (g.per[2] ? 0 : -1) : z + 1;
+    const int xs[3] = {xs0, x, xs2}, ys[3] = {ys0, y, ys2}, zs[3] = {zs0, z, zs2};
+    const bool on_face = (xs0 | xs2 | ys0 | ys2 | zs0 | zs2) < 0;
+    const bool near = (fl & F_NEAR) != 0;
+
+    uint32_t face = 0, bcp = 0, bcc = 0, mov = 0;
+    if (on_face || near) {
+#pragma unroll
+      for (int d = 0; d < 18; d++) {
+        const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
+        if ((sx | sy | sz) < 0) {
+          face |= 1u << d;
+        } else if (near) {
+          const uint8_t fs = flags[sx + nxl * sy + nxy * sz];
+          if (fs & F_SOLID_PREV) bcp |= 1u << d;
+          if (fs & F_SOLID) bcc |= 1u << d;
+          if (fs & F_MOVING) mov |= 1u << d;
+        }
+      }
+    }
+    const uint32_t bcr = face | bcp;  // incoming slots holding boundary values (read side)
+    const uint32_t bcw = face | bcc;  // incoming slots to fill with boundary values (write side)
+    const bool fresh = (fl & F_SOLID_PREV) != 0;
+
+    C pst[Q];
+    C rho, ux, uy, uz;
+    if (!fresh) {
+      C f[Q];
+#pragma unroll
+      for (int d = 0; d < Q; d++) {
+        long long a;
+        if (!ODD || d == 18) {
+          a = (long long)d * g.plane + i;
+        } else {
+          const long long src = xs[1 - cx(d)] + nxl * ys[1 - cy(d)] + nxy * zs[1 - cz(d)];
+          a = ((bcr >> d) & 1u) ? (long long)d * g.plane + i : (long long)opp(d) * g.plane + src;
+        }
+        f[d] = SP::ld(A + a, d, rho0);
+      }
+      moments<C, FORCE>(f, k, rho, ux, uy, uz);
+      collide<C, TRT, FORCE>(f, pst, k, rho, ux, uy, uz);
+    } else {
+      C mom[4];
+      fresh_state<C, TRT, FORCE>(k, p.kin, rho0, x, y, z, pst, mom);
+      rho = mom[0];
+      ux = mom[1];
+      uy = mom[2];
+      uz = mom[3];
+    }
+
+    // boundary value of incoming direction d (own slot A[d][x])
+    auto bcval = [&](const int d) -> C {
+      const int o = opp(d);
+      if ((face >> d) & 1u) {
+        // face of the missing source: x first, then y, then z (static indices only)
+        const bool xo = (cx(d) > 0 && xs0 < 0) || (cx(d) < 0 && xs2 < 0);
+        const bool yo = (cy(d) > 0 && ys0 < 0) || (cy(d) < 0 && ys2 < 0);
+        const int fx = cx(d) > 0 ? 0 : 1, fy = cy(d) > 0 ? 2 : 3, fz = cz(d) > 0 ? 4 : 5;
+        const int kind = xo ? p.face_kind[fx] : (yo ? p.face_kind[fy] : p.face_kind[fz]);
+        const C ufx = C(xo ? p.face_u[fx][0] : (yo ? p.face_u[fy][0] : p.face_u[fz][0]));
+        const C ufy = C(xo ? p.face_u[fx][1] : (yo ? p.face_u[fy][1] : p.face_u[fz][1]));
+        const C ufz = C(xo ? p.face_u[fx][2] : (yo ? p.face_u[fy][2] : p.face_u[fz][2]));
+        if (kind == LBM_FACE_EQ_INLET) return feq<C>(d, rho, ufx, ufy, ufz);
+        if (kind == LBM_FACE_OUTFLOW) return pst[d];
+        return pst[o] - C(6) * wgt<C>(o) * rho * cdot<C>(o, ufx, ufy, ufz);
+      }
+      C cdu = C(0);
+      if ((mov >> d) & 1u) {
+        double wx, wy, wz;
+        wall_velocity(p.kin, x + 0.5 + 0.5 * cx(o), y + 0.5 + 0.5 * cy(o), z + 0.5 + 0.5 * cz(o), wx,
+                      wy, wz);
+        cdu = cdot<C>(o, C(wx), C(wy), C(wz));
+      }
+      const C v = pst[o] - C(6) * wgt<C>(o) * rho * cdu;
+      if (p.compute_force) {
+        // momentum exchange of link (x, o): c_o (f*_o + f_in)
+        const double t = (double)pst[o] + (double)v;
+        const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
+        const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
+        const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
+        const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
+        acc[0] += fx;
+        acc[1] += fy;
+        acc[2] += fz;
+        acc[3] += ry * fz - rz * fy;
+        acc[4] += rz * fx - rx * fz;
+        acc[5] += rx * fy - ry * fx;
+        has_link = true;
+      }
+      return v;
+    };
+
+    if (!ODD) {
+#pragma unroll
+      for (int d = 0; d < Q; d++) {
+        C v;
+        if ((bcw >> d) & 1u) v = bcval(d);
+        else v = pst[opp(d)];
+        SP::st(A + (long long)d * g.plane + i, v, d, rho0);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < Q; j++) {
+        const int o = opp(j);
+        if ((bcw >> o) & 1u) {
+          // target x + c_j is outside/solid: the boundary value of incoming o goes to A[o][x]
+          const C v = bcval(o);
+          SP::st(A + (long long)o * g.plane + i, v, o, rho0);
+        } else if (j == 18 || !fresh || ((bcp >> o) & 1u)) {
+          // a fresh node leaves its emission toward old-fluid targets to them
+          const long long tgt = xs[1 + cx(j)] + nxl * ys[1 + cy(j)] + nxy * zs[1 + cz(j)];
+          SP::st(A + (long long)j * g.plane + tgt, pst[j], j, rho0);
+        }
+      }
+      if (!fresh) {
+        const uint32_t fnb = bcp & ~bcc & ~face;  // neighbours uncovered this step
+        if (fnb) {
+#pragma unroll
+          for (int d = 0; d < 18; d++) {
+            if (!((fnb >> d) & 1u)) continue;
+            // source coordinates of direction d (x - c_d), wrapped
+            const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
+            C q[Q], mom[4];
+            fresh_state<C, TRT, FORCE>(k, p.kin, rho0, sx, sy, sz, q, mom);
+            C qd = q[0];
+#pragma unroll
+            for (int e = 1; e < Q; e++)
+              if (e == d) qd = q[e];
+            SP::st(A + (long long)d * g.plane + i, qd, d, rho0);
+          }
+        }
+      }
+    }
+  }
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force);
+}
+
+// ---- state readout (populations, macros, mass, finiteness) ---------------------------
+// Reconstructs S_n[d, x] from the current layout using the flag bit `solid_bit`
+// (the flags of the last completed step).
+template <class SP>
+__device__ __forceinline__ void aa_read(const ReadParams& p, const typename SP::S* A, const uint8_t* flags,
+                                        int x, int y, int z, long long i, typename SP::C* f) {
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const C rho0 = C(p.rho0);
+  if (!p.swapped) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) f[d] = SP::ld(A + (long long)d * g.plane + i, d, rho0);
+    return;
+  }
+  const long long nxl = g.nx, nxy = (long long)g.nx * g.ny;
+  const int xs[3] = {x == 0 ? (g.per[0] ? g.nx - 1 : -1) : x - 1, x,
+                     x == g.nx - 1 ? (g.per[0] ? 0 : -1) : x + 1};
+  const int ys[3] = {y == 0 ? (g.per[1] ? g.ny - 1 : -1) : y - 1, y,
+                     y == g.ny - 1 ? (g.per[1] ? 0 : -1) : y + 1};
+  const int zs[3] = {z == 0 ? (g.per[2] ? g.nz - 1 : -1) : z - 1, z,
+                     z == g.nz - 1 ? (g.per[2] ? 0 : -1) : z + 1};
+#pragma unroll
+  for (int d = 0; d < Q; d++) {
+    long long a = (long long)d * g.plane + i;
+    if (d != 18) {
+      const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
+      if ((sx | sy | sz) >= 0) {
+        const long long src = sx + nxl * sy + nxy * sz;
+        if (!(flags[src] & p.solid_bit)) a = (long long)opp(d) * g.plane + src;
+      }
+    }
+    f[d] = SP::ld(A + a, d, rho0);
+  }
+}
+
+template <class SP>
+__global__ void aa_export_kernel(const ReadParams p, const typename SP::S* __restrict__ A,
+                                 const uint8_t* __restrict__ flags, ExportOut out) {
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const long long i = node_index(g, x, y, z);
+  C f[Q];
+  const bool solid = (flags[i] & p.solid_bit) != 0;
+  if (solid) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) f[d] = C(0);
+  } else {
+    aa_read<SP>(p, A, flags, x, y, z, i, f);
+  }
+  export_node<C>(out, g, i, f, solid, p.gacc);
+}
+
+template <class SP>
+__global__ void aa_reduce_kernel(const ReadParams p, const typename SP::S* __restrict__ A,
+                                 const uint8_t* __restrict__ flags, double* out) {
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  bool has = false;
+  if (x < g.nx && y < g.ny) {
+    const long long i = node_index(g, x, y, z);
+    if (!(flags[i] & p.solid_bit)) {
+      C f[Q];
+      aa_read<SP>(p, A, flags, x, y, z, i, f);
+      double m = 0.0;
+      bool bad = false;
+#pragma unroll
+      for (int d = 0; d < Q; d++) {
+        m += (double)f[d];
+        bad = bad || !isfinite((double)f[d]);
+      }
+      acc[0] = m;
+      acc[1] = bad ? 1.0 : 0.0;
+      has = true;
+    }
+  }
+  block_force_reduce(acc, has, out);
+}
+
+// ---- initial state ------------------------------------------------------------------------
+template <class SP>
+__global__ void aa_init_kernel(const InitParams p, typename SP::S* __restrict__ A,
+                               const uint8_t* __restrict__ flags) {
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const long long i = node_index(g, x, y, z);
+  const C rho0 = C(p.rho0);
+  const bool solid = (flags[i] & F_SOLID) != 0;
+  if (p.f_in) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) SP::st(A + (long long)d * g.plane + i, C(import_value(p, g, i, d)), d, rho0);
+    return;
+  }
+  const C r = p.rho ? C(p.rho[i]) : rho0;
+  const C u = p.u ? C(p.u[i]) : C(p.uni[0]);
+  const C v = p.v ? C(p.v[i]) : C(p.uni[1]);
+  const C w = p.w ? C(p.w[i]) : C(p.uni[2]);
+#pragma unroll
+  for (int d = 0; d < Q; d++)
+    SP::st(A + (long long)d * g.plane + i, solid ? C(0) : feq<C>(d, r, u, v, w), d, rho0);
+}
+
+// ---- host launchers ------------------------------------------------------------------------
+template <class SP, bool ODD, bool TRT, bool FORCE>
+static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, dim3 grid, dim3 block,
+                              cudaStream_t s) {
+  aa_step_kernel<SP, ODD, TRT, FORCE><<<grid, block, 0, s>>>(p, (typename SP::S*)A, flags);
+  return cudaGetLastError();
+}
+
+template <class SP>
+static cudaError_t launch_sp(const AAParams& p, void* A, const uint8_t* flags, bool odd, bool trt,
+                             bool force, dim3 grid, dim3 block, cudaStream_t s) {
+#define LBM_AA_CASE(O, T, F)                                                  \
+  if (odd == O && trt == T && force == F)                                     \
+    return launch_one<SP, O, T, F>(p, A, flags, grid, block, s);
+  LBM_AA_CASE(false, false, false)
+  LBM_AA_CASE(false, false, true)
+  LBM_AA_CASE(false, true, false)
+  LBM_AA_CASE(false, true, true)
+  LBM_AA_CASE(true, false, false)
+  LBM_AA_CASE(true, false, true)
+  LBM_AA_CASE(true, true, false)
+  LBM_AA_CASE(true, true, true)
+#undef LBM_AA_CASE
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t aa_launch_step(int storage, const AAParams& p, void* A, const uint8_t* flags, bool odd,
+                           bool trt, bool force, dim3 grid, dim3 block, cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32: return launch_sp<StF32>(p, A, flags, odd, trt, force, grid, block, s);
+    case LBM_STORE_FP64: return launch_sp<StF64>(p, A, flags, odd, trt, force, grid, block, s);
+    case LBM_STORE_FP16DEV: return launch_sp<StF16>(p, A, flags, odd, trt, force, grid, block, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
+                             const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32:
+      aa_export_kernel<StF32><<<grid, block, 0, s>>>(p, (const float*)A, flags, out);
+      break;
+    case LBM_STORE_FP64:
+      aa_export_kernel<StF64><<<grid, block, 0, s>>>(p, (const double*)A, flags, out);
+      break;
+    case LBM_STORE_FP16DEV:
+      aa_export_kernel<StF16><<<grid, block, 0, s>>>(p, (const __half*)A, flags, out);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
+                             double* out, dim3 grid, dim3 block, cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32:
+      aa_reduce_kernel<StF32><<<grid, block, 0, s>>>(p, (const float*)A, flags, out);
+      break;
+    case LBM_STORE_FP64:
+      aa_reduce_kernel<StF64><<<grid, block, 0, s>>>(p, (const double*)A, flags, out);
+      break;
+    case LBM_STORE_FP16DEV:
+      aa_reduce_kernel<StF16><<<grid, block, 0, s>>>(p, (const __half*)A, flags, out);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t aa_launch_init(int storage, const InitParams& p, void* A, const uint8_t* flags, dim3 grid,
+                           dim3 block, cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32: aa_init_kernel<StF32><<<grid, block, 0, s>>>(p, (float*)A, flags); break;
+    case LBM_STORE_FP64: aa_init_kernel<StF64><<<grid, block, 0, s>>>(p, (double*)A, flags); break;
+    case LBM_STORE_FP16DEV: aa_init_kernel<StF16><<<grid, block, 0, s>>>(p, (__half*)A, flags); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace lbm

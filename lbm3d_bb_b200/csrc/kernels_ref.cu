@@ -1,0 +1,408 @@
+// kernels_ref.cu — the reference step (MainCore.jl:245-379), fused into one kernel.
+//
+// The reference keeps two population arrays and runs, per step,
+//   collision! -> streaming! -> periodic_BC! -> solid_BC! -> velocity_BC!
+//   -> compute_aero! -> compute_macros!
+// with every node (solids included) collided and streamed.  Here the state
+// between steps is F = f*_{n-1} (post-collision) plus R = (rho, u, v, w) of
+// S_{n-1}; one kernel per step pulls S_n from F with the reference's wrap rules,
+// applies the solid bounce-back and the face conditions in registers, reduces the
+// momentum exchange, writes R_n (compute_macros!) and F_n = collide(S_n, R_n)
+// into the other buffer pair.
+//
+// This file is compiled with --fmad=false and keeps the reference's operation
+// order, so FP32 results round exactly as the reference kernels written in
+// plain Float32 arithmetic (no fused multiply-add) do.
+#include "lbm_internal.cuh"
+#include "lbm_kernels.h"
+
+namespace lbm {
+
+template <class T>
+struct RefT;
+template <>
+struct RefT<float> {
+  static __device__ __forceinline__ float W(int d) { return wgt<float>(d); }
+};
+template <>
+struct RefT<double> {
+  static __device__ __forceinline__ double W(int d) { return wgt<double>(d); }
+};
+
+// compute_macros!_gpu (ComputeMacro.jl:20-40): sequential sums from zero.
+template <class T>
+__device__ __forceinline__ void ref_moments(const T* S, T& rho, T& u, T& v, T& w) {
+  T r = T(0), mx = T(0), my = T(0), mz = T(0);
+#pragma unroll
+  for (int d = 0; d < Q; d++) {
+    const T f = S[d];
+    r += f;
+    mx += f * T(cx(d));
+    my += f * T(cy(d));
+    mz += f * T(cz(d));
+  }
+  rho = r;
+  u = mx / r;
+  v = my / r;
+  w = mz / r;
+}
+
+// BGK_collision!_gpu (Collision.jl:229-238) and TRT_collision!_gpu
+// (Collision.jl:136-170), statement for statement.
+template <class T, bool TRT>
+__device__ __forceinline__ void ref_collide(const T* S, T* F, T rho, T ux, T uy, T uz, T om_p, T om_m) {
+  if (!TRT) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      const T cu = T(cx(d)) * ux + T(cy(d)) * uy + T(cz(d)) * uz;
+      const T cu2 = cu * cu;
+      const T u2 = ux * ux + uy * uy + uz * uz;
+      const T fe = RefT<T>::W(d) * rho * (T(1) + cu * T(3) + T(0.5) * cu2 * T(9) - T(0.5) * u2 * T(3));
+      F[d] = S[d] - om_p * (S[d] - fe);
+    }
+  } else {
+    const T u2 = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      const T fi = S[d], fo = S[opp(d)];
+      const T cu = T(cx(d)) * ux + T(cy(d)) * uy + T(cz(d)) * uz;
+      const T cu2 = cu * cu;
+      const T fp_eq = RefT<T>::W(d) * rho * (T(1) + T(0.5) * cu2 * T(9) - T(0.5) * u2 * T(3));
+      const T fm_eq = RefT<T>::W(d) * rho * (cu * T(3));
+      const T fp = T(0.5) * (fi + fo);
+      const T fm = T(0.5) * (fi - fo);
+      const T fpn = fp - om_p * (fp - fp_eq);
+      const T fmn = fm - om_m * (fm - fm_eq);
+      F[d] = fpn + fmn;
+    }
+  }
+}
+
+// SBB!_gpu (SolidBC.jl:181-208) for link (x, dir): value of S[opp(dir)].
+template <class T>
+__device__ __forceinline__ T ref_sbb(const RefParams& p, T fdir, T rho_w, int x, int y, int dir);
+
+template <>
+__device__ __forceinline__ float ref_sbb<float>(const RefParams& p, float fdir, float rho_w, int x, int y,
+                                                int dir) {
+  const float h = p.h;
+  const float cxf = (float)cx(dir), cyf = (float)cy(dir);
+  const float xlat = (((float)(x + 1) - 0.5f) * h) / h;  // x_lli ./ h (MainCore.jl:199-200)
+  const float ylat = (((float)(y + 1) - 0.5f) * h) / h;
+  const float xw = xlat - 0.5f * cxf, yw = ylat - 0.5f * cyf;
+  const float rx = xw - (float)p.kin.center[0], ry = yw - (float)p.kin.center[1];
+  const float uwx = (float)p.kin.vel[0] - (float)p.kin.omega[2] * ry;
+  const float uwy = (float)p.kin.vel[1] + (float)p.kin.omega[2] * rx;
+  const float cdu = cxf * uwx + cyf * uwy;
+  return fdir - 2.0f * wgt<float>(dir) * rho_w * cdu * 3.0f;
+}
+
+template <>
+__device__ __forceinline__ double ref_sbb<double>(const RefParams& p, double fdir, double rho_w, int x,
+                                                  int y, int dir) {
+  const float h = p.h;
+  const double cxd = (double)cx(dir), cyd = (double)cy(dir);
+  const double xlat = (double)((((float)(x + 1) - 0.5f) * h) / h);
+  const double ylat = (double)((((float)(y + 1) - 0.5f) * h) / h);
+  const double xw = xlat - 0.5 * cxd, yw = ylat - 0.5 * cyd;
+  const double rx = xw - (double)(float)p.kin.center[0], ry = yw - (double)(float)p.kin.center[1];
+  const double uwx = (double)(float)p.kin.vel[0] - (double)(float)p.kin.omega[2] * ry;
+  const double uwy = (double)(float)p.kin.vel[1] + (double)(float)p.kin.omega[2] * rx;
+  const double cdu = cxd * uwx + cyd * uwy;
+  return fdir - 2.0 * wgt<double>(dir) * rho_w * cdu * 3.0;
+}
+
+// Pull S_n at node (x,y,z) from F_{n-1} and apply the solid and face conditions
+// (Streaming.jl:82-111, OtherBC.jl:65-82, SolidBC.jl:160-210, OtherBC.jl:112-169),
+// accumulating the momentum exchange (MEA.jl:93-113).
+template <class T>
+__device__ __forceinline__ void ref_pull(const RefParams& p, const T* __restrict__ Fp,
+                                         const T* __restrict__ Rp, const uint8_t* __restrict__ flags,
+                                         int x, int y, int z, long long i, T* S, double* acc, bool& has) {
+  const Grid& g = p.g;
+  const long long nxl = g.nx, nxy = (long long)g.nx * g.ny;
+  const int zm = z == 0 ? g.nz - 1 : z - 1, zp = z == g.nz - 1 ? 0 : z + 1;
+#pragma unroll
+  for (int d = 0; d < Q; d++) {
+    const int sx = x - cx(d), sy = y - cy(d);
+    const int sz = cz(d) == 1 ? zm : (cz(d) == -1 ? zp : z);
+    long long src = i;  // x/y out of domain: same node, same direction (Utilities.jl:773-776)
+    if (sx >= 0 && sx < g.nx && sy >= 0 && sy < g.ny) src = sx + nxl * sy + nxy * sz;
+    S[d] = Fp[(long long)d * g.plane + src];
+  }
+  const uint8_t fl = flags[i];
+  const bool solid = (fl & p.solid_bit) != 0;
+  const bool on_face = (x == 0) || (x == g.nx - 1) || (y == 0) || (y == g.ny - 1);
+  const bool near = !solid && (fl & F_NEAR);
+  if (!(near || on_face)) return;
+  const T rp = Rp[i];
+  uint32_t links = 0;
+  if (near) {
+#pragma unroll
+    for (int dir = 0; dir < Q; dir++) {
+      const int nx_ = x + cx(dir), ny_ = y + cy(dir), nz_ = z + cz(dir);
+      // nbr_lli: -1 outside the global domain, z included (Utilities.jl:559-569)
+      if (nx_ < 0 || nx_ >= g.nx || ny_ < 0 || ny_ >= g.ny || nz_ < 0 || nz_ >= g.nz) continue;
+      if (!(flags[nx_ + nxl * ny_ + nxy * nz_] & p.solid_bit)) continue;
+      links |= 1u << dir;
+      const T fdir = Fp[(long long)dir * g.plane + i];
+      S[opp(dir)] = ref_sbb<T>(p, fdir, rp, x, y, dir);
+    }
+  }
+  if (on_face) {
+    const T up = Rp[g.N + i], vp = Rp[2 * g.N + i], wp = Rp[3 * g.N + i];
+    const T U = T(p.U), V = T(p.V), W = T(p.W);
+    // velocity list: inlet x=1 (c_x>0), y=1 (c_y>0), y=Ny (c_y<0) — OtherBC.jl:139-148
+#pragma unroll
+    for (int dir = 0; dir < Q; dir++) {
+      const bool vel = (x == 0 && cx(dir) > 0) || (y == 0 && cy(dir) > 0) || (y == g.ny - 1 && cy(dir) < 0);
+      if (vel) {
+        const T cu = T(cx(dir)) * (-U) + T(cy(dir)) * (-V) + T(cz(dir)) * (-W);
+        S[dir] = Fp[(long long)opp(dir) * g.plane + i] - T(2) * RefT<T>::W(dir) * rp * cu * T(3);
+      }
+    }
+    // pressure list: outlet x=Nx (c_x<0) — OtherBC.jl:153-165; written last, so it
+    // wins where both lists name a slot
+    if (x == g.nx - 1) {
+#pragma unroll
+      for (int dir = 0; dir < Q; dir++) {
+        if (cx(dir) < 0) {
+          const T cu = T(cx(dir)) * up + T(cy(dir)) * vp + T(cz(dir)) * wp;
+          const T cu2 = cu * cu;
+          const T uu2 = up * up + vp * vp + wp * wp;
+          S[dir] = -Fp[(long long)opp(dir) * g.plane + i] +
+                   T(2) * RefT<T>::W(dir) * rp * (T(1) + T(0.5) * cu2 * T(9) - T(0.5) * uu2 * T(3));
+        }
+      }
+    }
+  }
+  if (links && p.compute_force) {
+    const double hl = (double)p.h;
+    const double rx = (double)((((float)(x + 1) - 0.5f) * p.h) / p.h) - (double)(float)p.kin.center[0];
+    const double ry = (double)((((float)(y + 1) - 0.5f) * p.h) / p.h) - (double)(float)p.kin.center[1];
+    const double rz = (z + 0.5) - p.kin.center[2];
+    (void)hl;
+#pragma unroll
+    for (int dir = 0; dir < Q; dir++) {
+      if (!((links >> dir) & 1u)) continue;
+      const double t = (double)Fp[(long long)dir * g.plane + i] + (double)S[opp(dir)];
+      const double fx = t * cx(dir), fy = t * cy(dir), fz = t * cz(dir);
+      acc[0] += fx;
+      acc[1] += fy;
+      acc[2] += fz;
+      acc[3] += ry * fz - rz * fy;
+      acc[4] += rz * fx - rx * fz;
+      acc[5] += rx * fy - ry * fx;
+    }
+    has = true;
+  }
+}
+
+template <class T, bool TRT>
+__global__ void __launch_bounds__(256) ref_step_kernel(const __grid_constant__ RefParams p,
+                                                       const T* __restrict__ Fp, const T* __restrict__ Rp,
+                                                       T* __restrict__ Fn, T* __restrict__ Rn,
+                                                       const uint8_t* __restrict__ flags) {
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  bool has = false;
+  if (p.zero_next && x == 0 && y == 0 && z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) p.zero_next[c] = 0.0;
+  }
+  if (x < g.nx && y < g.ny) {
+    const long long i = node_index(g, x, y, z);
+    T S[Q];
+    ref_pull<T>(p, Fp, Rp, flags, x, y, z, i, S, acc, has);
+    T rho, u, v, w;
+    ref_moments<T>(S, rho, u, v, w);
+    Rn[i] = rho;
+    Rn[g.N + i] = u;
+    Rn[2 * g.N + i] = v;
+    Rn[3 * g.N + i] = w;
+    T F[Q];
+    ref_collide<T, TRT>(S, F, rho, u, v, w, T(p.omega_p), T(p.omega_m));
+#pragma unroll
+    for (int d = 0; d < Q; d++) Fn[(long long)d * g.plane + i] = F[d];
+  }
+  if (p.compute_force) block_force_reduce(acc, has, p.force);
+}
+
+template <class T>
+__global__ void ref_export_kernel(const __grid_constant__ RefParams p, const T* __restrict__ Fp,
+                                  const T* __restrict__ Rp, int direct, const uint8_t* __restrict__ flags,
+                                  ExportOut out, double* mass) {
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  bool has = false;
+  if (x < g.nx && y < g.ny) {
+    const long long i = node_index(g, x, y, z);
+    T S[Q];
+    if (direct) {
+#pragma unroll
+      for (int d = 0; d < Q; d++) S[d] = Fp[(long long)d * g.plane + i];
+    } else {
+      double dummy[6] = {0, 0, 0, 0, 0, 0};
+      bool hd = false;
+      RefParams q = p;
+      q.compute_force = 0;
+      ref_pull<T>(q, Fp, Rp, flags, x, y, z, i, S, dummy, hd);
+    }
+    if (mass) {
+      double m = 0.0;
+      bool bad = false;
+#pragma unroll
+      for (int d = 0; d < Q; d++) {
+        m += (double)S[d];
+        bad = bad || !isfinite((double)S[d]);
+      }
+      acc[0] = m;
+      acc[1] = bad ? 1.0 : 0.0;
+      has = true;
+    } else {
+      const double zero3[3] = {0.0, 0.0, 0.0};
+      export_node<T>(out, g, i, S, false, zero3);
+    }
+  }
+  if (mass) block_force_reduce(acc, has, mass);
+}
+
+template <class T, bool TRT>
+__global__ void ref_prepare_kernel(const __grid_constant__ RefParams p, const T* __restrict__ S0,
+                                   T* __restrict__ F, T* __restrict__ R) {
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const long long i = node_index(g, x, y, z);
+  T S[Q];
+#pragma unroll
+  for (int d = 0; d < Q; d++) S[d] = S0[(long long)d * g.plane + i];
+  T rho, u, v, w;
+  ref_moments<T>(S, rho, u, v, w);
+  R[i] = rho;
+  R[g.N + i] = u;
+  R[2 * g.N + i] = v;
+  R[3 * g.N + i] = w;
+  T Fo[Q];
+  ref_collide<T, TRT>(S, Fo, rho, u, v, w, T(p.omega_p), T(p.omega_m));
+#pragma unroll
+  for (int d = 0; d < Q; d++) F[(long long)d * g.plane + i] = Fo[d];
+}
+
+// initialize_f_gpu (Initialization.jl:27-41) with the caller's velocity field.
+template <class T>
+__global__ void ref_init_kernel(const InitParams p, T* __restrict__ S) {
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const long long i = node_index(g, x, y, z);
+  if (p.f_in) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) S[(long long)d * g.plane + i] = T(import_value(p, g, i, d));
+    return;
+  }
+  const T r = p.rho ? T(p.rho[i]) : T(p.rho0);
+  const T ux = p.u ? T(p.u[i]) : T(p.uni[0]);
+  const T uy = p.v ? T(p.v[i]) : T(p.uni[1]);
+  const T uz = p.w ? T(p.w[i]) : T(p.uni[2]);
+#pragma unroll
+  for (int d = 0; d < Q; d++) {
+    const T cu = T(cx(d)) * ux + T(cy(d)) * uy + T(cz(d)) * uz;
+    const T u2 = ux * ux + uy * uy + uz * uz;
+    const T cu2 = cu * cu;
+    S[(long long)d * g.plane + i] =
+        RefT<T>::W(d) * r * (T(1) + cu * T(3) + T(0.5) * cu2 * T(9) - T(0.5) * u2 * T(3));
+  }
+}
+
+template <class T>
+__global__ void ref_macros_kernel(const Grid g, const T* __restrict__ R, ExportOut out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const long long i = node_index(g, x, y, z);
+  if (out.rho) put<T>(out.rho, i, out.m_dtype, R[i]);
+  if (out.u) put<T>(out.u, i, out.m_dtype, R[g.N + i]);
+  if (out.v) put<T>(out.v, i, out.m_dtype, R[2 * g.N + i]);
+  if (out.w) put<T>(out.w, i, out.m_dtype, R[3 * g.N + i]);
+}
+
+// ---- launchers --------------------------------------------------------------------
+cudaError_t ref_launch_step(bool fp64, bool trt, const RefParams& p, const void* Fp, const void* Rp,
+                            void* Fn, void* Rn, const uint8_t* flags, dim3 grid, dim3 block,
+                            cudaStream_t s) {
+  if (fp64) {
+    if (trt)
+      ref_step_kernel<double, true><<<grid, block, 0, s>>>(p, (const double*)Fp, (const double*)Rp,
+                                                           (double*)Fn, (double*)Rn, flags);
+    else
+      ref_step_kernel<double, false><<<grid, block, 0, s>>>(p, (const double*)Fp, (const double*)Rp,
+                                                            (double*)Fn, (double*)Rn, flags);
+  } else {
+    if (trt)
+      ref_step_kernel<float, true><<<grid, block, 0, s>>>(p, (const float*)Fp, (const float*)Rp,
+                                                          (float*)Fn, (float*)Rn, flags);
+    else
+      ref_step_kernel<float, false><<<grid, block, 0, s>>>(p, (const float*)Fp, (const float*)Rp,
+                                                           (float*)Fn, (float*)Rn, flags);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t ref_launch_export(bool fp64, const RefParams& p, const void* Fp, const void* Rp, int direct,
+                              const uint8_t* flags, const ExportOut& out, double* mass, dim3 grid,
+                              dim3 block, cudaStream_t s) {
+  if (fp64)
+    ref_export_kernel<double><<<grid, block, 0, s>>>(p, (const double*)Fp, (const double*)Rp, direct, flags,
+                                                     out, mass);
+  else
+    ref_export_kernel<float><<<grid, block, 0, s>>>(p, (const float*)Fp, (const float*)Rp, direct, flags,
+                                                    out, mass);
+  return cudaGetLastError();
+}
+
+cudaError_t ref_launch_prepare(bool fp64, bool trt, const RefParams& p, const void* S0, void* F, void* R,
+                               dim3 grid, dim3 block, cudaStream_t s) {
+  if (fp64) {
+    if (trt)
+      ref_prepare_kernel<double, true><<<grid, block, 0, s>>>(p, (const double*)S0, (double*)F, (double*)R);
+    else
+      ref_prepare_kernel<double, false><<<grid, block, 0, s>>>(p, (const double*)S0, (double*)F, (double*)R);
+  } else {
+    if (trt)
+      ref_prepare_kernel<float, true><<<grid, block, 0, s>>>(p, (const float*)S0, (float*)F, (float*)R);
+    else
+      ref_prepare_kernel<float, false><<<grid, block, 0, s>>>(p, (const float*)S0, (float*)F, (float*)R);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t ref_launch_init(bool fp64, const InitParams& p, void* S, dim3 grid, dim3 block, cudaStream_t s) {
+  if (fp64)
+    ref_init_kernel<double><<<grid, block, 0, s>>>(p, (double*)S);
+  else
+    ref_init_kernel<float><<<grid, block, 0, s>>>(p, (float*)S);
+  return cudaGetLastError();
+}
+
+cudaError_t ref_launch_macros(bool fp64, const Grid& g, const void* R, const ExportOut& out, dim3 grid,
+                              dim3 block, cudaStream_t s) {
+  if (fp64)
+    ref_macros_kernel<double><<<grid, block, 0, s>>>(g, (const double*)R, out);
+  else
+    ref_macros_kernel<float><<<grid, block, 0, s>>>(g, (const float*)R, out);
+  return cudaGetLastError();
+}
+
+}  // namespace lbm

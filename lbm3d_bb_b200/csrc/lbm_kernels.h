@@ -1,0 +1,191 @@
+// lbm_kernels.h — kernel parameter blocks and host launchers of liblbm3d.
+#pragma once
+
+#include "lbm_internal.cuh"
+
+namespace lbm {
+
+// Config-mode (AA) step.
+struct AAParams {
+  Grid g;
+  int face_kind[6];
+  double face_u[6][3];
+  double omega_p, omega_m, rho0;
+  double gacc[3];
+  Kinematics kin;
+  int compute_force;
+  double* force;      // 6 doubles of this step
+  double* zero_next;  // 6 doubles of the next step, cleared by this launch (may be null)
+};
+
+// Reference-mode step (two population buffers, virtual-fluid solids).
+struct RefParams {
+  Grid g;
+  float omega_p, omega_m;
+  float U, V, W;  // U_inf, V_inf, W_inf
+  float h;
+  Kinematics kin;  // lattice-unit half-step kinematics (Motion.jl:96-100), FP32-valued
+  uint8_t solid_bit;
+  int compute_force;
+  double* force;
+  double* zero_next;
+};
+
+// Read-back of the state of the last completed step.
+struct ReadParams {
+  Grid g;
+  double rho0;
+  int swapped;        // AA: state in swapped layout (after an even phase)
+  uint8_t solid_bit;  // flag bit holding the solids of the last completed step
+  double gacc[3];
+};
+
+struct ExportOut {
+  void* f;  // populations (nullable)
+  int f_dtype, f_layout;
+  void* rho;  // macros (nullable)
+  void* u;
+  void* v;
+  void* w;
+  int m_dtype;
+};
+
+struct InitParams {
+  Grid g;
+  double rho0;
+  double uni[3];
+  const double* rho;  // device arrays (nullable)
+  const double* u;
+  const double* v;
+  const double* w;
+  const void* f_in;  // device populations to import (nullable)
+  int f_dtype, f_layout;
+};
+
+template <class T>
+__device__ __forceinline__ void put(void* base, long long k, int dtype, T v) {
+  if (dtype == LBM_DTYPE_F64)
+    ((double*)base)[k] = (double)v;
+  else
+    ((float*)base)[k] = (float)v;
+}
+
+__device__ __forceinline__ double import_value(const InitParams& p, const Grid& g, long long i, int d) {
+  const long long k = p.f_layout == LBM_LAYOUT_SOA ? (long long)d * g.N + i : (long long)d + 19LL * i;
+  return p.f_dtype == LBM_DTYPE_F64 ? ((const double*)p.f_in)[k] : (double)((const float*)p.f_in)[k];
+}
+
+// Writes one node's populations and/or moments (config-mode moments: u = j/rho + g/2).
+template <class C>
+__device__ __forceinline__ void export_node(const ExportOut& o, const Grid& g, long long i, const C* f,
+                                            bool solid, const double* gacc) {
+  if (o.f) {
+#pragma unroll
+    for (int d = 0; d < 19; d++) {
+      const long long k = o.f_layout == LBM_LAYOUT_SOA ? (long long)d * g.N + i : (long long)d + 19LL * i;
+      put<C>(o.f, k, o.f_dtype, f[d]);
+    }
+  }
+  if (o.rho || o.u || o.v || o.w) {
+    C r = f[0], jx = C(0), jy = C(0), jz = C(0);
+#pragma unroll
+    for (int d = 1; d < 19; d++) r += f[d];
+#pragma unroll
+    for (int d = 0; d < 19; d++) {
+      jx += f[d] * C(cx(d));
+      jy += f[d] * C(cy(d));
+      jz += f[d] * C(cz(d));
+    }
+    C ux = C(0), uy = C(0), uz = C(0);
+    if (!solid) {
+      ux = jx / r + C(0.5) * C(gacc[0]);
+      uy = jy / r + C(0.5) * C(gacc[1]);
+      uz = jz / r + C(0.5) * C(gacc[2]);
+    } else {
+      r = C(0);
+    }
+    if (o.rho) put<C>(o.rho, i, o.m_dtype, r);
+    if (o.u) put<C>(o.u, i, o.m_dtype, ux);
+    if (o.v) put<C>(o.v, i, o.m_dtype, uy);
+    if (o.w) put<C>(o.w, i, o.m_dtype, uz);
+  }
+}
+
+// Block reduction of the six force/torque components; one FP64 atomic each.
+__device__ __forceinline__ void block_force_reduce(double* acc, bool has, double* out) {
+  __shared__ double red[32][6];
+  const int nthreads = blockDim.x * blockDim.y;
+  if (!__syncthreads_or(has)) return;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    double v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][k] = v;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int nw = (nthreads + 31) >> 5;
+    for (int k = 0; k < 6; k++) {
+      double s = 0.0;
+      for (int w = 0; w < nw; w++) s += red[w][k];
+      atomicAdd(out + k, s);
+    }
+  }
+}
+
+// ---- launchers (kernels_aa.cu) ----
+cudaError_t aa_launch_step(int storage, const AAParams& p, void* A, const uint8_t* flags, bool odd,
+                           bool trt, bool force, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
+                             const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
+                             double* out, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t aa_launch_init(int storage, const InitParams& p, void* A, const uint8_t* flags, dim3 grid,
+                           dim3 block, cudaStream_t s);
+
+// ---- launchers (kernels_ref.cu) ----
+// Fp/Rp: post-collision populations and macros of the previous state; Fn/Rn: outputs.
+cudaError_t ref_launch_step(bool fp64, bool trt, const RefParams& p, const void* Fp, const void* Rp,
+                            void* Fn, void* Rn, const uint8_t* flags, dim3 grid, dim3 block,
+                            cudaStream_t s);
+// S_n export (pull of Fp with Rp), or direct export of a stored S (direct != 0).
+cudaError_t ref_launch_export(bool fp64, const RefParams& p, const void* Fp, const void* Rp, int direct,
+                              const uint8_t* flags, const ExportOut& out, double* mass, dim3 grid,
+                              dim3 block, cudaStream_t s);
+// From S (pre-collision, SoA in the context's precision) compute R = moments(S)
+// and F = collide(S, R) (the state the next step pulls from).
+cudaError_t ref_launch_prepare(bool fp64, bool trt, const RefParams& p, const void* Sdirect, void* F,
+                               void* R, dim3 grid, dim3 block, cudaStream_t s);
+// S = feq_ref(rho, u) or imported populations, in the context's precision.
+cudaError_t ref_launch_init(bool fp64, const InitParams& p, void* S, dim3 grid, dim3 block, cudaStream_t s);
+// Copies the stored macros R (4 planes) into caller arrays.
+cudaError_t ref_launch_macros(bool fp64, const Grid& g, const void* R, const ExportOut& out, dim3 grid,
+                              dim3 block, cudaStream_t s);
+
+// ---- geometry (geometry.cu) ----
+struct FlagParams {
+  Grid g;
+  int mode;       // LBM_MODE_*
+  Box box;        // region (unwrapped coordinates; wrapped on periodic axes)
+  BodyDev body;   // moving body
+  BodyDev body_prev;  // same body at the pose of the last completed step
+  int has_moving;
+};
+cudaError_t geo_launch_static(const Grid& g, const BodyDev& b, const Box& box, uint8_t* flags,
+                              cudaStream_t s);
+cudaError_t geo_launch_spheres(const Grid& g, const double* xyzr, int count, uint8_t* flags,
+                               cudaStream_t s);
+cudaError_t geo_launch_moving(const FlagParams& p, uint8_t* flags, cudaStream_t s);
+cudaError_t geo_launch_near(const Grid& g, int mode, const Box& box, uint8_t* flags, cudaStream_t s);
+cudaError_t geo_launch_sync_prev(const Grid& g, uint8_t* flags, cudaStream_t s);
+// Link export: counts per node (cur solid bits), exclusive scan, CSR fill.
+cudaError_t geo_links(const Grid& g, int mode, const uint8_t* flags, uint8_t solid_bit, int32_t* d_count,
+                      long long* d_scan, long long* d_blocksums, int32_t* d_ptr, int32_t* d_lidx,
+                      int8_t* d_dirs, long long cap, long long* h_nnz, cudaStream_t s);
+cudaError_t geo_masks(const Grid& g, int mode, const uint8_t* flags, uint8_t solid_bit, uint8_t* ms,
+                      uint8_t* mb, cudaStream_t s);
+
+}  // namespace lbm
