@@ -217,6 +217,9 @@ int32_t lbm_set_populations(lbm_ctx* ctx, const void* f, int32_t dtype, int32_t 
 int32_t lbm_step(lbm_ctx* ctx, int32_t nsteps);
 /* Completed steps since initialisation. */
 int64_t lbm_step_count(const lbm_ctx* ctx);
+/* Kernels launched by lbm_step on this context so far (step kernels and the
+ * moving-body flag kernels); no reference counterpart. */
+int64_t lbm_launch_count(const lbm_ctx* ctx);
 
 /* ---- outputs ------------------------------------------------------------------ */
 /* Replaces compute_aero!'s reduction (MEA.jl:30-54): momentum-exchange force

@@ -55,6 +55,7 @@ def lib() -> C.CDLL:
         "lbm_set_populations": (i32, [vp, vp, i32, i32, i32]),
         "lbm_step": (i32, [vp, i32]),
         "lbm_step_count": (i64, [vp]),
+        "lbm_launch_count": (i64, [vp]),
         "lbm_get_force": (i32, [vp, i64, vp]),
         "lbm_get_force_history": (i32, [vp, i64, i32, vp]),
         "lbm_get_macros": (i32, [vp, vp, vp, vp, vp, i32, i32]),
@@ -80,7 +81,7 @@ def exported_symbols() -> list[str]:
         "lbm_abi_version", "lbm_status_string", "lbm_global_error", "lbm_read_params", "lbm_lattice",
         "lbm_create", "lbm_destroy", "lbm_last_error", "lbm_set_stream", "lbm_synchronize",
         "lbm_device_bytes", "lbm_set_launch", "lbm_get_launch", "lbm_add_body", "lbm_add_spheres",
-        "lbm_update_body", "lbm_init_equilibrium", "lbm_set_populations", "lbm_step", "lbm_step_count",
+        "lbm_update_body", "lbm_init_equilibrium", "lbm_set_populations", "lbm_step", "lbm_step_count", "lbm_launch_count",
         "lbm_get_force", "lbm_get_force_history", "lbm_get_macros", "lbm_get_populations", "lbm_get_flags",
         "lbm_get_links", "lbm_mass", "lbm_check",
     ]

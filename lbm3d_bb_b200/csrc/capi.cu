@@ -51,10 +51,11 @@ struct lbm_ctx {
   bool ref_direct = false;  // reference: F[1-ri] holds S_n itself (no step since init)
   bool swapped = false;     // config: state in swapped layout (next phase odd)
   uint8_t* flags = nullptr;
-  double* ring = nullptr;  // (cap + 1) slots of 6 doubles
+  double* ring = nullptr;  // (cap + 1) force records of FORCE_RECORD doubles
   int ring_slots = 0;
   double* scratch = nullptr;  // 8 doubles
   long long nstep = 0;
+  long long launches = 0;  // kernels this context has launched
   bool initialised = false;
   size_t bytes = 0;
   // bodies
@@ -233,10 +234,12 @@ int sync_flags(lbm_ctx* c) {
     p.body = to_dev(c, b, &c->pose_latest);
     p.body_prev = to_dev(c, b, &c->pose_last_step);
     p.has_moving = 1;
+    c->launches++;
     int rc = c->cuda(geo_launch_moving(p, c->flags, c->stream), "moving-body flags");
     if (rc) return rc;
   }
   if (box_clamp(c, rn)) {
+    c->launches++;
     int rc = c->cuda(geo_launch_near(c->g, c->cfg.mode, rn, c->flags, c->stream), "near flags");
     if (rc) return rc;
   }
@@ -604,12 +607,12 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
   }
   if (c->cuda(cudaMalloc(&c->flags, fl), "cudaMalloc(flags)")) return bail(LBM_ERR_CUDA);
   c->ring_slots = c->cfg.force_history + 1;
-  if (c->cuda(cudaMalloc(&c->ring, (size_t)c->ring_slots * 6 * sizeof(double)), "cudaMalloc(force ring)"))
-    return bail(LBM_ERR_CUDA);
+  const size_t ring_bytes = (size_t)c->ring_slots * FORCE_RECORD * sizeof(double);
+  if (c->cuda(cudaMalloc(&c->ring, ring_bytes), "cudaMalloc(force ring)")) return bail(LBM_ERR_CUDA);
   if (c->cuda(cudaMalloc(&c->scratch, 8 * sizeof(double)), "cudaMalloc(scratch)")) return bail(LBM_ERR_CUDA);
-  c->bytes += fl + (size_t)c->ring_slots * 48 + 64;
+  c->bytes += fl + ring_bytes + 64;
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);
-  if (c->cuda(cudaMemset(c->ring, 0, (size_t)c->ring_slots * 48), "memset ring")) return bail(LBM_ERR_CUDA);
+  if (c->cuda(cudaMemset(c->ring, 0, ring_bytes), "memset ring")) return bail(LBM_ERR_CUDA);
   if (c->A && c->cuda(cudaMemset(c->A, 0, pop), "memset populations")) return bail(LBM_ERR_CUDA);
   *out = c;
   return LBM_OK;
@@ -769,7 +772,9 @@ int32_t lbm_init_equilibrium(lbm_ctx* c, const double* rho, const double* u, con
   }
   c->nstep = 0;
   c->initialised = true;
-  if (c->cuda(cudaMemsetAsync(c->ring, 0, (size_t)c->ring_slots * 48, c->stream), "memset ring")) return LBM_ERR_CUDA;
+  if (c->cuda(cudaMemsetAsync(c->ring, 0, (size_t)c->ring_slots * FORCE_RECORD * sizeof(double), c->stream),
+              "memset ring"))
+    return LBM_ERR_CUDA;
   return c->cuda(cudaStreamSynchronize(c->stream), "init");
 }
 
@@ -818,14 +823,15 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
     int rc = sync_flags(c);
     if (rc) return rc;
     const long long step = c->nstep + 1;  // 1-based step number being computed
-    double* slot = c->ring + (size_t)(step % c->ring_slots) * 6;
-    double* next = c->ring + (size_t)((step + 1) % c->ring_slots) * 6;
+    double* slot = c->ring + (size_t)(step % c->ring_slots) * FORCE_RECORD;
+    double* next = c->ring + (size_t)((step + 1) % c->ring_slots) * FORCE_RECORD;
     if (c->ref) {
       RefParams p = ref_params(c, c->kin_latest, F_SOLID);
       p.compute_force = c->cfg.compute_force ? 1 : 0;
       p.force = slot;
       p.zero_next = next;
       for (int a = 0; a < 3; a++) p.kin.center[a] = c->kin_latest.center[a];
+      c->launches++;
       rc = c->cuda(ref_launch_step(is_ref_fp64(c), trt, p, c->F[c->ri], c->R[c->ri], c->F[1 - c->ri], c->R[1 - c->ri],
                                    c->flags, c->grid(), c->block(), c->stream),
                    "reference step");
@@ -849,7 +855,21 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
       p.compute_force = c->cfg.compute_force ? 1 : 0;
       p.force = slot;
       p.zero_next = next;
+      {
+        const long long nx = c->g.nx, nxy = (long long)c->g.nx * c->g.ny, pl = c->g.plane;
+        for (int d = 0; d < 19; d++) {
+          const long long nb = cx(d) + nx * cy(d) + nxy * cz(d);
+          if (!c->swapped) {  // even phase: own slots
+            p.off_rd[d] = d * pl;
+            p.off_wr[d] = d * pl;
+          } else {  // odd phase: pull from x - c_d (slot opp(d)), push to x + c_d (slot d)
+            p.off_rd[d] = opp(d) * pl - nb;
+            p.off_wr[d] = d * pl + nb;
+          }
+        }
+      }
       const bool force = c->cfg.accel[0] != 0.0 || c->cfg.accel[1] != 0.0 || c->cfg.accel[2] != 0.0;
+      c->launches++;
       rc = c->cuda(aa_launch_step(c->cfg.storage, p, c->A, c->flags, c->swapped, trt, force, c->grid(), c->block(),
                                   c->stream),
                    "AA step");
@@ -865,20 +885,30 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
 
 int64_t lbm_step_count(const lbm_ctx* c) { return c ? c->nstep : -1; }
 
+int64_t lbm_launch_count(const lbm_ctx* c) { return c ? c->launches : -1; }
+
 int32_t lbm_get_force_history(lbm_ctx* c, int64_t first, int32_t count, double* out) {
   if (!c || !out || count < 0) return LBM_ERR_ARG;
   if (first < 1 || first + count - 1 > c->nstep || c->nstep - first + 1 > c->cfg.force_history)
     return c->fail(LBM_ERR_ARG, "steps %lld..%lld not in the force history (last %d of %lld steps)", (long long)first,
                    (long long)(first + count - 1), c->cfg.force_history, (long long)c->nstep);
   if (c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  std::vector<double> rec((size_t)count * FORCE_RECORD);
   for (int32_t k = 0; k < count; k++) {
     const long long s = first + k;
-    if (c->cuda(cudaMemcpyAsync(out + 6 * (size_t)k, c->ring + (size_t)(s % c->ring_slots) * 6, 48,
-                                cudaMemcpyDeviceToHost, c->stream),
+    if (c->cuda(cudaMemcpyAsync(rec.data() + (size_t)k * FORCE_RECORD, c->ring + (size_t)(s % c->ring_slots) * FORCE_RECORD,
+                                FORCE_RECORD * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
                 "D2H force"))
       return LBM_ERR_CUDA;
   }
-  return c->cuda(cudaStreamSynchronize(c->stream), "force");
+  if (c->cuda(cudaStreamSynchronize(c->stream), "force")) return LBM_ERR_CUDA;
+  for (int32_t k = 0; k < count; k++)
+    for (int j = 0; j < 6; j++) {
+      double sum = 0.0;
+      for (int l = 0; l < FORCE_SLOTS; l++) sum += rec[(size_t)k * FORCE_RECORD + 8 * l + j];
+      out[6 * (size_t)k + j] = sum;
+    }
+  return LBM_OK;
 }
 
 int32_t lbm_get_force(lbm_ctx* c, int64_t step, double out[6]) { return lbm_get_force_history(c, step, 1, out); }

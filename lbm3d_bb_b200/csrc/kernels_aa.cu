@@ -34,12 +34,14 @@ namespace lbm {
 struct StF32 {
   using S = float;
   using C = float;
+  static constexpr int MIN_BLOCKS = 4;  // 256 x 4 threads -> at most 64 registers
   static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
   static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
 };
 struct StF64 {
   using S = double;
   using C = double;
+  static constexpr int MIN_BLOCKS = 2;
   static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
   static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
 };
@@ -47,6 +49,7 @@ struct StF64 {
 struct StF16 {
   using S = __half;
   using C = float;
+  static constexpr int MIN_BLOCKS = 4;
   static __device__ __forceinline__ C ld(const S* p, int d, C rho0) {
     return wgt<float>(d) * rho0 + __half2float(*p);
   }
@@ -200,11 +203,206 @@ __device__ __noinline__ void fresh_state(Coll<C> k, Kinematics kin, C rho0, int 
 }
 
 // ---- the step kernel ------------------------------------------------------------------
+// General path of one fluid node: faces, solid links, moving-body refill, momentum
+// exchange.  Kept out of line so that its register demand does not limit the
+// occupancy of the interior fast path; only warps containing a boundary node run it.
 template <class SP, bool ODD, bool TRT, bool FORCE>
-__global__ void __launch_bounds__(256) aa_step_kernel(const __grid_constant__ AAParams p, typename SP::S* __restrict__ A,
-                                                      const uint8_t* __restrict__ flags) {
+__device__ __noinline__ void aa_general(const AAParams& p, typename SP::S* __restrict__ A,
+                                        const uint8_t* __restrict__ flags, const int x, const int y,
+                                        const int z, const long long i, const uint8_t fl, double* acc,
+                                        bool* has_out) {
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const C rho0 = C(p.rho0);
+  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
+  bool has_link = false;
+  const long long nxl = g.nx, nxy = (long long)g.nx * g.ny;
+  // neighbour coordinates; -1 when outside a non-periodic axis
+  const int xs0 = x == 0 ? (g.per[0] ? g.nx - 1 : -1) : x - 1;
+  const int xs2 = x == g.nx - 1 ? (g.per[0] ? 0 : -1) : x + 1;
+  const int ys0 = y == 0 ? (g.per[1] ? g.ny - 1 : -1) : y - 1;
+  const int ys2 = y == g.ny - 1 ? (g.per[1] ? 0 : -1) : y + 1;
+  const int zs0 = z == 0 ? (g.per[2] ? g.nz - 1 : -1) : z - 1;
+  const int zs2 = z == g.nz - 1 ? (g.per[2] ? 0 : -1) : z + 1;
+  const int xs[3] = {xs0, x, xs2}, ys[3] = {ys0, y, ys2}, zs[3] = {zs0, z, zs2};
+  const bool on_face = (xs0 | xs2 | ys0 | ys2 | zs0 | zs2) < 0;
+  const bool near = (fl & F_NEAR) != 0;
+
+  uint32_t face = 0, bcp = 0, bcc = 0, mov = 0;
+  if (on_face || near) {
+#pragma unroll
+    for (int d = 0; d < 18; d++) {
+      const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
+      if ((sx | sy | sz) < 0) {
+        face |= 1u << d;
+      } else if (near) {
+        const uint8_t fs = flags[sx + nxl * sy + nxy * sz];
+        if (fs & F_SOLID_PREV) bcp |= 1u << d;
+        if (fs & F_SOLID) bcc |= 1u << d;
+        if (fs & F_MOVING) mov |= 1u << d;
+      }
+    }
+  }
+  const uint32_t bcr = face | bcp;  // incoming slots holding boundary values (read side)
+  const uint32_t bcw = face | bcc;  // incoming slots to fill with boundary values (write side)
+  const bool fresh = (fl & F_SOLID_PREV) != 0;
+
+  C pst[Q];
+  C rho, ux, uy, uz;
+  if (!fresh) {
+    C f[Q];
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      long long a;
+      if (!ODD || d == 18) {
+        a = (long long)d * g.plane + i;
+      } else {
+        const long long src = xs[1 - cx(d)] + nxl * ys[1 - cy(d)] + nxy * zs[1 - cz(d)];
+        a = ((bcr >> d) & 1u) ? (long long)d * g.plane + i : (long long)opp(d) * g.plane + src;
+      }
+      f[d] = SP::ld(A + a, d, rho0);
+    }
+    moments<C, FORCE>(f, k, rho, ux, uy, uz);
+    collide<C, TRT, FORCE>(f, pst, k, rho, ux, uy, uz);
+  } else {
+    C mom[4];
+    fresh_state<C, TRT, FORCE>(k, p.kin, rho0, x, y, z, pst, mom);
+    rho = mom[0];
+    ux = mom[1];
+    uy = mom[2];
+    uz = mom[3];
+  }
+
+  // boundary value of incoming direction d (own slot A[d][x])
+  auto bcval = [&](const int d) -> C {
+    const int o = opp(d);
+    if ((face >> d) & 1u) {
+      // face of the missing source: x first, then y, then z (static indices only)
+      const bool xo = (cx(d) > 0 && xs0 < 0) || (cx(d) < 0 && xs2 < 0);
+      const bool yo = (cy(d) > 0 && ys0 < 0) || (cy(d) < 0 && ys2 < 0);
+      const int fx = cx(d) > 0 ? 0 : 1, fy = cy(d) > 0 ? 2 : 3, fz = cz(d) > 0 ? 4 : 5;
+      const int kind = xo ? p.face_kind[fx] : (yo ? p.face_kind[fy] : p.face_kind[fz]);
+      const C ufx = C(xo ? p.face_u[fx][0] : (yo ? p.face_u[fy][0] : p.face_u[fz][0]));
+      const C ufy = C(xo ? p.face_u[fx][1] : (yo ? p.face_u[fy][1] : p.face_u[fz][1]));
+      const C ufz = C(xo ? p.face_u[fx][2] : (yo ? p.face_u[fy][2] : p.face_u[fz][2]));
+      if (kind == LBM_FACE_EQ_INLET) return feq<C>(d, rho, ufx, ufy, ufz);
+      if (kind == LBM_FACE_OUTFLOW) return pst[d];
+      return pst[o] - C(6) * wgt<C>(o) * rho * cdot<C>(o, ufx, ufy, ufz);
+    }
+    C cdu = C(0);
+    if ((mov >> d) & 1u) {
+      double wx, wy, wz;
+      wall_velocity(p.kin, x + 0.5 + 0.5 * cx(o), y + 0.5 + 0.5 * cy(o), z + 0.5 + 0.5 * cz(o), wx,
+                    wy, wz);
+      cdu = cdot<C>(o, C(wx), C(wy), C(wz));
+    }
+    const C v = pst[o] - C(6) * wgt<C>(o) * rho * cdu;
+    if (p.compute_force) {
+      // momentum exchange of link (x, o): c_o (f*_o + f_in)
+      const double t = (double)pst[o] + (double)v;
+      const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
+      const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
+      const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
+      const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
+      acc[0] += fx;
+      acc[1] += fy;
+      acc[2] += fz;
+      acc[3] += ry * fz - rz * fy;
+      acc[4] += rz * fx - rx * fz;
+      acc[5] += rx * fy - ry * fx;
+      has_link = true;
+    }
+    return v;
+  };
+
+  if (!ODD) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      C v;
+      if ((bcw >> d) & 1u) v = bcval(d);
+      else v = pst[opp(d)];
+      SP::st(A + (long long)d * g.plane + i, v, d, rho0);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+      const int o = opp(j);
+      if ((bcw >> o) & 1u) {
+        // target x + c_j is outside/solid: the boundary value of incoming o goes to A[o][x]
+        const C v = bcval(o);
+        SP::st(A + (long long)o * g.plane + i, v, o, rho0);
+      } else if (j == 18 || !fresh || ((bcp >> o) & 1u)) {
+        // a fresh node leaves its emission toward old-fluid targets to them
+        const long long tgt = xs[1 + cx(j)] + nxl * ys[1 + cy(j)] + nxy * zs[1 + cz(j)];
+        SP::st(A + (long long)j * g.plane + tgt, pst[j], j, rho0);
+      }
+    }
+    if (!fresh) {
+      const uint32_t fnb = bcp & ~bcc & ~face;  // neighbours uncovered this step
+      if (fnb) {
+#pragma unroll
+        for (int d = 0; d < 18; d++) {
+          if (!((fnb >> d) & 1u)) continue;
+          // source coordinates of direction d (x - c_d), wrapped
+          const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
+          C q[Q], mom[4];
+          fresh_state<C, TRT, FORCE>(k, p.kin, rho0, sx, sy, sz, q, mom);
+          C qd = q[0];
+#pragma unroll
+          for (int e = 1; e < Q; e++)
+            if (e == d) qd = q[e];
+          SP::st(A + (long long)d * g.plane + i, qd, d, rho0);
+        }
+      }
+    }
+  }
+  *has_out = has_link;
+}
+
+// Interior fast path: no boundary in reach, neighbour offsets precomputed on the
+// host (p.off_rd / p.off_wr); only the periodic x wrap is patched per lane.
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__device__ __forceinline__ void aa_fast(const AAParams& p, typename SP::S* __restrict__ A, const long long i,
+                                        const int x) {
   using S = typename SP::S;
   using C = typename SP::C;
+  const C rho0 = C(p.rho0);
+  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
+  S* const base = A + i;
+  long long fix_lo = 0, fix_hi = 0;  // periodic x wrap at the row ends (odd phase)
+  if (ODD) {
+    fix_lo = x == 0 ? (long long)p.g.nx : 0;
+    fix_hi = x == p.g.nx - 1 ? (long long)p.g.nx : 0;
+  }
+  C f[Q];
+#pragma unroll
+  for (int d = 0; d < Q; d++) {
+    long long o = p.off_rd[d];
+    if (ODD) {
+      if (cx(d) == 1) o += fix_lo;
+      if (cx(d) == -1) o -= fix_hi;
+    }
+    f[d] = SP::ld(base + o, d, rho0);
+  }
+  C rho, ux, uy, uz;
+  moments<C, FORCE>(f, k, rho, ux, uy, uz);
+  C pst[Q];
+  collide<C, TRT, FORCE>(f, pst, k, rho, ux, uy, uz);
+#pragma unroll
+  for (int j = 0; j < Q; j++) {
+    long long o = p.off_wr[j];
+    if (ODD) {
+      if (cx(j) == 1) o -= fix_hi;
+      if (cx(j) == -1) o += fix_lo;
+    }
+    SP::st(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
+  }
+}
+
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __grid_constant__ AAParams p,
+                                                                      typename SP::S* __restrict__ A,
+                                                                      const uint8_t* __restrict__ flags) {
   const Grid& g = p.g;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -212,160 +410,29 @@ __global__ void __launch_bounds__(256) aa_step_kernel(const __grid_constant__ AA
   const bool inb = (x < g.nx) && (y < g.ny);
   const long long i = inb ? node_index(g, x, y, z) : 0;
   const uint8_t fl = inb ? flags[i] : (uint8_t)F_SOLID;
+  const bool solid = (fl & F_SOLID) != 0;
+
+  clear_record(p.zero_next);  // the next step's force record (read by the next launch only)
+
+  // A lane may take the fast path when no boundary is in reach: not NEAR, not on a
+  // non-periodic face, and (odd phase) no y/z wrap.
+  const bool xin = g.per[0] || (x > 0 && x < g.nx - 1);
+  bool fast = !(fl & F_NEAR) && xin;
+  if (ODD) {
+    fast = fast && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
+  } else {
+    fast = fast && (g.per[1] || (y > 0 && y < g.ny - 1)) && (g.per[2] || (z > 0 && z < g.nz - 1));
+  }
+  const bool warp_fast = __all_sync(0xffffffffu, solid || fast);
+
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool has_link = false;
-  const C rho0 = C(p.rho0);
-  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
-
-  if (p.zero_next && x == 0 && y == 0 && z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
-    // clear the force slot of the next step (read by the next launch only)
-#pragma unroll
-    for (int c = 0; c < 6; c++) p.zero_next[c] = 0.0;
+  if (warp_fast) {
+    if (!solid) aa_fast<SP, ODD, TRT, FORCE>(p, A, i, x);
+  } else if (!solid) {
+    aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, i, fl, acc, &has_link);
   }
-
-  if (!(fl & F_SOLID)) {
-    const long long nxl = g.nx, nxy = (long long)g.nx * g.ny;
-    // neighbour coordinates; -1 when outside a non-periodic axis
-    const int xs0 = x == 0 ? (g.per[0] ? g.nx - 1 : -1) : x - 1;
-    const int xs2 = x == g.nx - 1 ? (g.per[0] ? 0 : -1) : x + 1;
-    const int ys0 = y == 0 ? (g.per[1] ? g.ny - 1 : -1) : y - 1;
-    const int ys2 = y == g.ny - 1 ? (g.per[1] ? 0 : -1) : y + 1;
-    const int zs0 = z == 0 ? (g.per[2] ? g.nz - 1 : -1) : z - 1;
-    const int zs2 = z == g.nz - 1 ? (g.per[2] ? 0 : -1) : z + 1;
-    const int xs[3] = {xs0, x, xs2}, ys[3] = {ys0, y, ys2}, zs[3] = {zs0, z, zs2};
-    const bool on_face = (xs0 | xs2 | ys0 | ys2 | zs0 | zs2) < 0;
-    const bool near = (fl & F_NEAR) != 0;
-
-    uint32_t face = 0, bcp = 0, bcc = 0, mov = 0;
-    if (on_face || near) {
-#pragma unroll
-      for (int d = 0; d < 18; d++) {
-        const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
-        if ((sx | sy | sz) < 0) {
-          face |= 1u << d;
-        } else if (near) {
-          const uint8_t fs = flags[sx + nxl * sy + nxy * sz];
-          if (fs & F_SOLID_PREV) bcp |= 1u << d;
-          if (fs & F_SOLID) bcc |= 1u << d;
-          if (fs & F_MOVING) mov |= 1u << d;
-        }
-      }
-    }
-    const uint32_t bcr = face | bcp;  // incoming slots holding boundary values (read side)
-    const uint32_t bcw = face | bcc;  // incoming slots to fill with boundary values (write side)
-    const bool fresh = (fl & F_SOLID_PREV) != 0;
-
-    C pst[Q];
-    C rho, ux, uy, uz;
-    if (!fresh) {
-      C f[Q];
-#pragma unroll
-      for (int d = 0; d < Q; d++) {
-        long long a;
-        if (!ODD || d == 18) {
-          a = (long long)d * g.plane + i;
-        } else {
-          const long long src = xs[1 - cx(d)] + nxl * ys[1 - cy(d)] + nxy * zs[1 - cz(d)];
-          a = ((bcr >> d) & 1u) ? (long long)d * g.plane + i : (long long)opp(d) * g.plane + src;
-        }
-        f[d] = SP::ld(A + a, d, rho0);
-      }
-      moments<C, FORCE>(f, k, rho, ux, uy, uz);
-      collide<C, TRT, FORCE>(f, pst, k, rho, ux, uy, uz);
-    } else {
-      C mom[4];
-      fresh_state<C, TRT, FORCE>(k, p.kin, rho0, x, y, z, pst, mom);
-      rho = mom[0];
-      ux = mom[1];
-      uy = mom[2];
-      uz = mom[3];
-    }
-
-    // boundary value of incoming direction d (own slot A[d][x])
-    auto bcval = [&](const int d) -> C {
-      const int o = opp(d);
-      if ((face >> d) & 1u) {
-        // face of the missing source: x first, then y, then z (static indices only)
-        const bool xo = (cx(d) > 0 && xs0 < 0) || (cx(d) < 0 && xs2 < 0);
-        const bool yo = (cy(d) > 0 && ys0 < 0) || (cy(d) < 0 && ys2 < 0);
-        const int fx = cx(d) > 0 ? 0 : 1, fy = cy(d) > 0 ? 2 : 3, fz = cz(d) > 0 ? 4 : 5;
-        const int kind = xo ? p.face_kind[fx] : (yo ? p.face_kind[fy] : p.face_kind[fz]);
-        const C ufx = C(xo ? p.face_u[fx][0] : (yo ? p.face_u[fy][0] : p.face_u[fz][0]));
-        const C ufy = C(xo ? p.face_u[fx][1] : (yo ? p.face_u[fy][1] : p.face_u[fz][1]));
-        const C ufz = C(xo ? p.face_u[fx][2] : (yo ? p.face_u[fy][2] : p.face_u[fz][2]));
-        if (kind == LBM_FACE_EQ_INLET) return feq<C>(d, rho, ufx, ufy, ufz);
-        if (kind == LBM_FACE_OUTFLOW) return pst[d];
-        return pst[o] - C(6) * wgt<C>(o) * rho * cdot<C>(o, ufx, ufy, ufz);
-      }
-      C cdu = C(0);
-      if ((mov >> d) & 1u) {
-        double wx, wy, wz;
-        wall_velocity(p.kin, x + 0.5 + 0.5 * cx(o), y + 0.5 + 0.5 * cy(o), z + 0.5 + 0.5 * cz(o), wx,
-                      wy, wz);
-        cdu = cdot<C>(o, C(wx), C(wy), C(wz));
-      }
-      const C v = pst[o] - C(6) * wgt<C>(o) * rho * cdu;
-      if (p.compute_force) {
-        // momentum exchange of link (x, o): c_o (f*_o + f_in)
-        const double t = (double)pst[o] + (double)v;
-        const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
-        const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
-        const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
-        const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
-        acc[0] += fx;
-        acc[1] += fy;
-        acc[2] += fz;
-        acc[3] += ry * fz - rz * fy;
-        acc[4] += rz * fx - rx * fz;
-        acc[5] += rx * fy - ry * fx;
-        has_link = true;
-      }
-      return v;
-    };
-
-    if (!ODD) {
-#pragma unroll
-      for (int d = 0; d < Q; d++) {
-        C v;
-        if ((bcw >> d) & 1u) v = bcval(d);
-        else v = pst[opp(d)];
-        SP::st(A + (long long)d * g.plane + i, v, d, rho0);
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < Q; j++) {
-        const int o = opp(j);
-        if ((bcw >> o) & 1u) {
-          // target x + c_j is outside/solid: the boundary value of incoming o goes to A[o][x]
-          const C v = bcval(o);
-          SP::st(A + (long long)o * g.plane + i, v, o, rho0);
-        } else if (j == 18 || !fresh || ((bcp >> o) & 1u)) {
-          // a fresh node leaves its emission toward old-fluid targets to them
-          const long long tgt = xs[1 + cx(j)] + nxl * ys[1 + cy(j)] + nxy * zs[1 + cz(j)];
-          SP::st(A + (long long)j * g.plane + tgt, pst[j], j, rho0);
-        }
-      }
-      if (!fresh) {
-        const uint32_t fnb = bcp & ~bcc & ~face;  // neighbours uncovered this step
-        if (fnb) {
-#pragma unroll
-          for (int d = 0; d < 18; d++) {
-            if (!((fnb >> d) & 1u)) continue;
-            // source coordinates of direction d (x - c_d), wrapped
-            const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
-            C q[Q], mom[4];
-            fresh_state<C, TRT, FORCE>(k, p.kin, rho0, sx, sy, sz, q, mom);
-            C qd = q[0];
-#pragma unroll
-            for (int e = 1; e < Q; e++)
-              if (e == d) qd = q[e];
-            SP::st(A + (long long)d * g.plane + i, qd, d, rho0);
-          }
-        }
-      }
-    }
-  }
-  if (p.compute_force) block_force_reduce(acc, has_link, p.force);
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
 // ---- state readout (populations, macros, mass, finiteness) ---------------------------

@@ -209,10 +209,7 @@ __global__ void __launch_bounds__(256) ref_step_kernel(const __grid_constant__ R
   const int z = blockIdx.z;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   bool has = false;
-  if (p.zero_next && x == 0 && y == 0 && z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
-#pragma unroll
-    for (int c = 0; c < 6; c++) p.zero_next[c] = 0.0;
-  }
+  clear_record(p.zero_next);  // the next step's force record (read by the next launch only)
   if (x < g.nx && y < g.ny) {
     const long long i = node_index(g, x, y, z);
     T S[Q];
@@ -228,7 +225,7 @@ __global__ void __launch_bounds__(256) ref_step_kernel(const __grid_constant__ R
 #pragma unroll
     for (int d = 0; d < Q; d++) Fn[(long long)d * g.plane + i] = F[d];
   }
-  if (p.compute_force) block_force_reduce(acc, has, p.force);
+  if (p.compute_force) block_force_reduce(acc, has, p.force + block_stripe());
 }
 
 template <class T>

@@ -15,7 +15,11 @@ struct AAParams {
   Kinematics kin;
   int compute_force;
   double* force;      // 6 doubles of this step
-  double* zero_next;  // 6 doubles of the next step, cleared by this launch (may be null)
+  double* zero_next;  // force record of the next step, cleared by this launch (may be null)
+  // interior fast path: element offsets, relative to the node, of the 19 reads and
+  // the 19 writes of this phase (even: own slots; odd: neighbour slots)
+  long long off_rd[19];
+  long long off_wr[19];
 };
 
 // Reference-mode step (two population buffers, virtual-fluid solids).
@@ -109,6 +113,24 @@ __device__ __forceinline__ void export_node(const ExportOut& o, const Grid& g, l
     if (o.v) put<C>(o.v, i, o.m_dtype, uy);
     if (o.w) put<C>(o.w, i, o.m_dtype, uz);
   }
+}
+
+// A step's force record: FORCE_SLOTS cache lines of 8 doubles (F, T, pad); each
+// block adds into line (block index mod FORCE_SLOTS) so that same-address FP64
+// atomics spread over many L2 lines.  The host sums the lines.
+constexpr int FORCE_SLOTS = 32;
+constexpr int FORCE_RECORD = FORCE_SLOTS * 8;  // doubles per step
+
+__device__ __forceinline__ int block_stripe() {
+  const unsigned b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  return (int)(b % FORCE_SLOTS) * 8;
+}
+
+// Clears the next step's force record (block 0 only; read by the next launch).
+__device__ __forceinline__ void clear_record(double* rec) {
+  if (rec == nullptr || (blockIdx.x | blockIdx.y | blockIdx.z) != 0) return;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  for (int t = tid; t < FORCE_RECORD; t += blockDim.x * blockDim.y) rec[t] = 0.0;
 }
 
 // Block reduction of the six force/torque components; one FP64 atomic each.

@@ -132,6 +132,10 @@ class Domain:
     def step_count(self) -> int:
         return int(self._L.lbm_step_count(self._h))
 
+    @property
+    def launch_count(self) -> int:
+        return int(self._L.lbm_launch_count(self._h))
+
     # -- outputs ----------------------------------------------------------------------------
     def force(self, step: Optional[int] = None) -> np.ndarray:
         out = np.zeros(6, dtype=np.float64)
