@@ -51,6 +51,13 @@ struct lbm_ctx {
   bool ref_direct = false;  // reference: F[1-ri] holds S_n itself (no step since init)
   bool swapped = false;     // config: state in swapped layout (next phase odd)
   uint8_t* flags = nullptr;
+  // TMA-staged step (config mode): per-tile boundary bits and the pipeline error word
+  bool tma = false;
+  int tma_tw = 0, tma_stages = 0;
+  long long ntiles = 0;
+  uint8_t* tiles = nullptr;
+  bool tiles_dirty = true;
+  int* d_err = nullptr;
   double* ring = nullptr;  // (cap + 1) force records of FORCE_RECORD doubles
   int ring_slots = 0;
   double* scratch = nullptr;  // 8 doubles
@@ -245,6 +252,7 @@ int sync_flags(lbm_ctx* c) {
   }
   c->pose_bits_prev = c->pose_last_step;
   c->pose_bits_cur = c->pose_latest;
+  c->tiles_dirty = true;
   return LBM_OK;
 }
 
@@ -354,6 +362,7 @@ int reduce_state(lbm_ctx* c, double out[2]) {
 }
 
 int near_full(lbm_ctx* c) {
+  c->tiles_dirty = true;
   Box f = full_box(c);
   return c->cuda(geo_launch_near(c->g, c->cfg.mode, f, c->flags, c->stream), "near flags");
 }
@@ -610,6 +619,23 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
   const size_t ring_bytes = (size_t)c->ring_slots * FORCE_RECORD * sizeof(double);
   if (c->cuda(cudaMalloc(&c->ring, ring_bytes), "cudaMalloc(force ring)")) return bail(LBM_ERR_CUDA);
   if (c->cuda(cudaMalloc(&c->scratch, 8 * sizeof(double)), "cudaMalloc(scratch)")) return bail(LBM_ERR_CUDA);
+  if (c->cuda(cudaMalloc(&c->d_err, sizeof(int)), "cudaMalloc(err)")) return bail(LBM_ERR_CUDA);
+  if (c->cuda(cudaMemset(c->d_err, 0, sizeof(int)), "memset err")) return bail(LBM_ERR_CUDA);
+  // TMA-staged step: rows split into 128-cell tiles with 16-byte aligned segments
+  {
+    const char* off = std::getenv("LBM3D_NO_TMA");
+    const int tw = 128;
+    if (!c->ref && !(off && off[0] == '1') && cfg->nx % tw == 0 && (cfg->nx * (long long)c->elem) % 16 == 0) {
+      c->tma = true;
+      c->tma_tw = tw;
+      c->ntiles = c->g.N / tw;
+      c->tma_stages = cfg->storage == LBM_STORE_FP64 ? 3 : (cfg->storage == LBM_STORE_FP16DEV ? 6 : 4);
+      const char* st = std::getenv("LBM3D_TMA_STAGES");
+      if (st && std::atoi(st) >= 2 && std::atoi(st) <= 8) c->tma_stages = std::atoi(st);
+      if (c->cuda(cudaMalloc(&c->tiles, (size_t)c->ntiles), "cudaMalloc(tiles)")) return bail(LBM_ERR_CUDA);
+      c->bytes += (size_t)c->ntiles;
+    }
+  }
   c->bytes += fl + ring_bytes + 64;
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);
   if (c->cuda(cudaMemset(c->ring, 0, ring_bytes), "memset ring")) return bail(LBM_ERR_CUDA);
@@ -630,6 +656,8 @@ int32_t lbm_destroy(lbm_ctx* c) {
   cudaFree(c->flags);
   cudaFree(c->ring);
   cudaFree(c->scratch);
+  cudaFree(c->d_err);
+  cudaFree(c->tiles);
   delete c;
   return LBM_OK;
 }
@@ -642,9 +670,19 @@ int32_t lbm_set_stream(lbm_ctx* c, void* stream) {
   return LBM_OK;
 }
 
+// Reads the device error word the step kernels set when a pipeline wait gives up.
+static int pipeline_status(lbm_ctx* c) {
+  int h = 0;
+  if (c->cuda(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H err")) return LBM_ERR_CUDA;
+  if (c->cuda(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize")) return LBM_ERR_CUDA;
+  if (h) return c->fail(LBM_ERR_CUDA, "a TMA pipeline wait in the step kernel gave up (error word %d)", h);
+  return LBM_OK;
+}
+
 int32_t lbm_synchronize(lbm_ctx* c) {
   if (!c) return LBM_ERR_ARG;
-  return c->cuda(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  if (c->cuda(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize")) return LBM_ERR_CUDA;
+  return pipeline_status(c);
 }
 
 int64_t lbm_device_bytes(const lbm_ctx* c) { return c ? (int64_t)c->bytes : 0; }
@@ -868,6 +906,25 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
           }
         }
       }
+      if (c->tma) {
+        if (c->tiles_dirty) {
+          c->launches++;
+          rc = c->cuda(aa_launch_tile_flags(c->g, c->tma_tw, c->ntiles, c->flags, c->tiles, c->stream), "tile flags");
+          if (rc) return rc;
+          c->tiles_dirty = false;
+        }
+        TmaCfg& T = p.tma;
+        T.enabled = 1;
+        T.tw = c->tma_tw;
+        T.halo = (int)(16 / c->elem);
+        T.ntx = c->g.nx / c->tma_tw;
+        T.ntiles = c->ntiles;
+        T.stages = c->tma_stages;
+        T.buf_elems = T.tw + T.halo;
+        T.stage_bytes = (int)(((size_t)19 * T.buf_elems * c->elem + 127) / 128 * 128);
+        T.tile_slow = c->tiles;
+        T.err = c->d_err;
+      }
       const bool force = c->cfg.accel[0] != 0.0 || c->cfg.accel[1] != 0.0 || c->cfg.accel[2] != 0.0;
       c->launches++;
       rc = c->cuda(aa_launch_step(c->cfg.storage, p, c->A, c->flags, c->swapped, trt, force, c->grid(), c->block(),
@@ -1051,7 +1108,7 @@ int32_t lbm_check(lbm_ctx* c) {
   int rc = reduce_state(c, r);
   if (rc) return rc;
   if (r[1] != 0.0) return c->fail(LBM_ERR_NUMERIC, "%.0f nodes hold non-finite populations", r[1]);
-  return LBM_OK;
+  return pipeline_status(c);
 }
 
 }  // extern "C"

@@ -28,13 +28,17 @@
 #include "lbm_internal.cuh"
 #include "lbm_kernels.h"
 
+#ifndef LBM_MINB_F32
+#define LBM_MINB_F32 4
+#endif
+
 namespace lbm {
 
 // ---- storage policies ------------------------------------------------------------
 struct StF32 {
   using S = float;
   using C = float;
-  static constexpr int MIN_BLOCKS = 4;  // 256 x 4 threads -> at most 64 registers
+  static constexpr int MIN_BLOCKS = LBM_MINB_F32;  // 256 x 4 threads -> at most 64 registers
   static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
   static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
 };
@@ -49,7 +53,7 @@ struct StF64 {
 struct StF16 {
   using S = __half;
   using C = float;
-  static constexpr int MIN_BLOCKS = 4;
+  static constexpr int MIN_BLOCKS = LBM_MINB_F32;
   static __device__ __forceinline__ C ld(const S* p, int d, C rho0) {
     return wgt<float>(d) * rho0 + __half2float(*p);
   }
@@ -65,23 +69,39 @@ struct Coll {
   C gx, gy, gz;  // body acceleration
 };
 
-// Moments of f: rho, j, then u = j/rho + g/2 (Guo).  Sums run in direction
-// order with the zero terms of c_d skipped.
+// 1/rho: one MUFU instruction in FP32 (rho is O(1), the ~1 ulp error is far below
+// the storage precision); exact division in FP64.
+__device__ __forceinline__ float recip(float r) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(r));
+  return y;
+}
+__device__ __forceinline__ double recip(double r) { return 1.0 / r; }
+
+// Moments from the nine opposite-direction pairs (d, d+1): s = f_d + f_{d+1},
+// t = f_d - f_{d+1}; rho = sum s + f_18, j = sum over pairs of c_d t.  Then
+// u = j/rho + g/2 (Guo).
 template <class C, bool FORCE>
 __device__ __forceinline__ void moments(const C* f, const Coll<C>& k, C& rho, C& ux, C& uy, C& uz) {
-  C r = f[0], jx = C(0), jy = C(0), jz = C(0);
+  C sp[9], tp[9];
 #pragma unroll
-  for (int d = 1; d < Q; d++) r += f[d];
-#pragma unroll
-  for (int d = 0; d < Q; d++) {
-    if (cx(d) == 1) jx += f[d];
-    if (cx(d) == -1) jx -= f[d];
-    if (cy(d) == 1) jy += f[d];
-    if (cy(d) == -1) jy -= f[d];
-    if (cz(d) == 1) jz += f[d];
-    if (cz(d) == -1) jz -= f[d];
+  for (int q = 0; q < 9; q++) {
+    sp[q] = f[2 * q] + f[2 * q + 1];
+    tp[q] = f[2 * q] - f[2 * q + 1];
   }
-  C inv = C(1) / r;
+  C r = ((sp[0] + sp[1]) + (sp[2] + sp[3])) + ((sp[4] + sp[5]) + (sp[6] + sp[7])) + (sp[8] + f[18]);
+  C jx = C(0), jy = C(0), jz = C(0);
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    const int d = 2 * q;
+    if (cx(d) == 1) jx += tp[q];
+    if (cx(d) == -1) jx -= tp[q];
+    if (cy(d) == 1) jy += tp[q];
+    if (cy(d) == -1) jy -= tp[q];
+    if (cz(d) == 1) jz += tp[q];
+    if (cz(d) == -1) jz -= tp[q];
+  }
+  const C inv = recip(r);
   rho = r;
   ux = jx * inv;
   uy = jy * inv;
@@ -112,64 +132,75 @@ __device__ __forceinline__ C feq(int d, C rho, C ux, C uy, C uz) {
   return wgt<C>(d) * rho * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * usq);
 }
 
-// BGK / TRT with Guo forcing; f -> p (post-collision).
+// BGK / TRT with Guo forcing, f -> p, written per opposite pair (d, d+1) with
+// c_{d+1} = -c_d: the equilibrium splits into an even part
+// e = w rho (1 - 1.5 u^2 + 4.5 (c.u)^2) and an odd part o = 3 w rho (c.u), the Guo
+// source S_d = w [3 (c_d - u).F + 9 (c_d.u)(c_d.F)] into w (9 (c.u)(c.F) - 3 u.F) and
+// 3 w (c.F).  Relaxation rates and weights are folded per weight class.
 template <class C, bool TRT, bool FORCE>
 __device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rho, C ux, C uy, C uz) {
   const C usq = ux * ux + uy * uy + uz * uz;
   const C base = C(1) - C(1.5) * usq;
-  C Fx = C(0), Fy = C(0), Fz = C(0), uF = C(0);
+  C Fx = C(0), Fy = C(0), Fz = C(0), m3uF = C(0);
   if (FORCE) {
     Fx = rho * k.gx;
     Fy = rho * k.gy;
     Fz = rho * k.gz;
-    uF = ux * Fx + uy * Fy + uz * Fz;
+    m3uF = C(-3) * (ux * Fx + uy * Fy + uz * Fz);
   }
+  const C wr1 = rho * wgt<C>(0), wr2 = rho * wgt<C>(6), wr0 = rho * wgt<C>(18);
   if (!TRT) {
-    const C fac = C(1) - C(0.5) * k.om_p;
+    const C om = k.om_p, omc = C(1) - k.om_p;
+    // omega * e = B + T (c.u)^2 ; omega * o = O (c.u)
+    const C B1 = om * wr1 * base, B2 = om * wr2 * base;
+    const C T1 = C(4.5) * om * wr1, T2 = C(4.5) * om * wr2;
+    const C O1 = C(3) * om * wr1, O2 = C(3) * om * wr2;
+    const C fac = C(1) - C(0.5) * om;
+    const C G1 = fac * wgt<C>(0), G2 = fac * wgt<C>(6);
 #pragma unroll
-    for (int d = 0; d < Q; d++) {
-      const C wr = wgt<C>(d) * rho;
+    for (int q = 0; q < 9; q++) {
+      const int d = 2 * q;
+      const bool c1 = d < 6;
       const C cu = cdot<C>(d, ux, uy, uz);
-      const C fe = wr * (base + cu * (C(3) + C(4.5) * cu));
-      C v = f[d] - k.om_p * (f[d] - fe);
+      C e = (c1 ? T1 : T2) * (cu * cu) + (c1 ? B1 : B2);
+      C o = (c1 ? O1 : O2) * cu;
       if (FORCE) {
         const C cF = cdot<C>(d, Fx, Fy, Fz);
-        v += fac * wgt<C>(d) * (C(3) * (cF - uF) + C(9) * cu * cF);
+        const C G = c1 ? G1 : G2;
+        e += G * (C(9) * (cu * cF) + m3uF);
+        o += (C(3) * G) * cF;
       }
-      p[d] = v;
+      p[d] = omc * f[d] + (e + o);
+      p[d + 1] = omc * f[d + 1] + (e - o);
     }
+    C e0 = om * wr0 * base;
+    if (FORCE) e0 += fac * wgt<C>(18) * m3uF;
+    p[18] = omc * f[18] + e0;
   } else {
-    const C fac_p = C(1) - C(0.5) * k.om_p, fac_m = C(1) - C(0.5) * k.om_m;
+    const C hp = C(0.5) * k.om_p, hm = C(0.5) * k.om_m;
+    const C fac_p = C(1) - hp, fac_m = C(1) - hm;
 #pragma unroll
-    for (int d = 0; d < 18; d += 2) {
-      const int o = d + 1;
-      const C wr = wgt<C>(d) * rho;
+    for (int q = 0; q < 9; q++) {
+      const int d = 2 * q;
+      const C wr = d < 6 ? wr1 : wr2;
       const C cu = cdot<C>(d, ux, uy, uz);
-      const C ep = wr * (base + C(4.5) * cu * cu);
-      const C em = wr * (C(3) * cu);
-      const C fp = C(0.5) * (f[d] + f[o]);
-      const C fm = C(0.5) * (f[d] - f[o]);
-      C rp = k.om_p * (fp - ep);
-      C rm = k.om_m * (fm - em);
-      C a = f[d] - rp - rm;
-      C b = f[o] - rp + rm;
+      C e = wr * (base + C(4.5) * (cu * cu));
+      C o = (C(3) * wr) * cu;
+      // A = om_p (f+ - e), Bm = om_m (f- - o), f+- = (f_d +- f_d+1)/2
+      C A = hp * (f[d] + f[d + 1]) - k.om_p * e;
+      C Bm = hm * (f[d] - f[d + 1]) - k.om_m * o;
       if (FORCE) {
+        const C w = wgt<C>(d);
         const C cF = cdot<C>(d, Fx, Fy, Fz);
-        const C sp = wgt<C>(d) * (C(9) * cu * cF - C(3) * uF);
-        const C sm = wgt<C>(d) * (C(3) * cF);
-        a += fac_p * sp + fac_m * sm;
-        b += fac_p * sp - fac_m * sm;
+        A -= fac_p * w * (C(9) * (cu * cF) + m3uF);
+        Bm -= fac_m * (C(3) * w) * cF;
       }
-      p[d] = a;
-      p[o] = b;
+      p[d] = (f[d] - A) - Bm;
+      p[d + 1] = (f[d + 1] - A) + Bm;
     }
-    {
-      const C wr = wgt<C>(18) * rho;
-      const C ep = wr * base;
-      C v = f[18] - k.om_p * (f[18] - ep);
-      if (FORCE) v += fac_p * wgt<C>(18) * (C(-3) * uF);
-      p[18] = v;
-    }
+    C v = f[18] - k.om_p * (f[18] - wr0 * base);
+    if (FORCE) v += fac_p * wgt<C>(18) * m3uF;
+    p[18] = v;
   }
 }
 
@@ -356,7 +387,7 @@ __device__ __noinline__ void aa_general(const AAParams& p, typename SP::S* __res
       }
     }
   }
-  *has_out = has_link;
+  *has_out = *has_out || has_link;
 }
 
 // Interior fast path: no boundary in reach, neighbour offsets precomputed on the
@@ -399,21 +430,17 @@ __device__ __forceinline__ void aa_fast(const AAParams& p, typename SP::S* __res
   }
 }
 
+// One node on the direct path: warps with no boundary in reach take the fast path,
+// others the general path.  Lanes of a warp must belong to the same launch shape
+// (all 32 lanes reach the vote).
 template <class SP, bool ODD, bool TRT, bool FORCE>
-__global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __grid_constant__ AAParams p,
-                                                                      typename SP::S* __restrict__ A,
-                                                                      const uint8_t* __restrict__ flags) {
+__device__ __forceinline__ void aa_direct(const AAParams& p, typename SP::S* __restrict__ A,
+                                          const uint8_t* __restrict__ flags, const int x, const int y, const int z,
+                                          const bool inb, double* acc, bool* has_link) {
   const Grid& g = p.g;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const bool inb = (x < g.nx) && (y < g.ny);
   const long long i = inb ? node_index(g, x, y, z) : 0;
   const uint8_t fl = inb ? flags[i] : (uint8_t)F_SOLID;
   const bool solid = (fl & F_SOLID) != 0;
-
-  clear_record(p.zero_next);  // the next step's force record (read by the next launch only)
-
   // A lane may take the fast path when no boundary is in reach: not NEAR, not on a
   // non-periodic face, and (odd phase) no y/z wrap.
   const bool xin = g.per[0] || (x > 0 && x < g.nx - 1);
@@ -424,13 +451,201 @@ __global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __gr
     fast = fast && (g.per[1] || (y > 0 && y < g.ny - 1)) && (g.per[2] || (z > 0 && z < g.nz - 1));
   }
   const bool warp_fast = __all_sync(0xffffffffu, solid || fast);
-
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  bool has_link = false;
   if (warp_fast) {
     if (!solid) aa_fast<SP, ODD, TRT, FORCE>(p, A, i, x);
   } else if (!solid) {
-    aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, i, fl, acc, &has_link);
+    aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, i, fl, acc, has_link);
+  }
+}
+
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __grid_constant__ AAParams p,
+                                                                      typename SP::S* __restrict__ A,
+                                                                      const uint8_t* __restrict__ flags) {
+  const Grid& g = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = (x < g.nx) && (y < g.ny);
+  clear_record(p.zero_next);  // the next step's force record (read by the next launch only)
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  aa_direct<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, inb, acc, &has_link);
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
+}
+
+// ---- TMA-staged persistent step ------------------------------------------------------
+// Tiles are row segments of TW cells.  For every tile without a boundary node, one
+// thread streams the 19 direction segments it needs (even phase: the node's own
+// slots; odd phase: the neighbour slots, row-shifted, plus a 16-byte halo for the
+// x-shifted directions) into shared memory with cp.async.bulk, several tiles ahead,
+// completion tracked by one mbarrier per stage.  The compute reads shared memory,
+// so loads stay in flight while warps compute.  Tiles holding a boundary node are
+// processed by the direct path.
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// Bounded wait on an mbarrier phase: gives up after ~2^22 polls (each try_wait
+// blocks for a hardware-defined interval), returning false.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 22); it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+constexpr int TMA_MAX_STAGES = 8;
+
+template <class SP, bool ODD>
+__device__ __forceinline__ void tma_issue(const AAParams& p, const typename SP::S* A, long long tile,
+                                          unsigned char* stage, uint32_t bar) {
+  using S = typename SP::S;
+  const Grid& g = p.g;
+  const TmaCfg& T = p.tma;
+  const int tw = T.tw, H = T.halo;
+  const long long row = tile / T.ntx;
+  const int x0 = (int)(tile - row * T.ntx) * tw;
+  const int y = (int)(row % g.ny), z = (int)(row / g.ny);
+  const uint32_t seg = (uint32_t)(tw * sizeof(S)), hal = 16u;
+  mbar_expect_tx(bar, ODD ? 19u * seg + 10u * hal : 19u * seg);
+  const uint32_t dst0 = smem_u32(stage);
+  const uint32_t dstride = (uint32_t)(T.buf_elems * sizeof(S));
+#pragma unroll 1
+  for (int d = 0; d < Q; d++) {
+    const uint32_t dst = dst0 + d * dstride;
+    if (!ODD) {
+      bulk_g2s(dst, A + (long long)d * g.plane + row * g.nx + x0, seg, bar);
+      continue;
+    }
+    int ys = y - cy(d), zs = z - cz(d);
+    ys = ys < 0 ? ys + g.ny : (ys >= g.ny ? ys - g.ny : ys);
+    zs = zs < 0 ? zs + g.nz : (zs >= g.nz ? zs - g.nz : zs);
+    const S* rowp = A + (long long)opp(d) * g.plane + ((long long)zs * g.ny + ys) * g.nx;
+    const int c = cx(d);
+    if (c == 0) {
+      bulk_g2s(dst, rowp + x0, seg, bar);
+    } else if (c == 1) {  // source x-1: [halo | main]
+      bulk_g2s(dst, rowp + (x0 >= H ? x0 - H : g.nx - H), hal, bar);
+      bulk_g2s(dst + hal, rowp + x0, seg, bar);
+    } else {  // source x+1: [main | halo]
+      bulk_g2s(dst, rowp + x0, seg, bar);
+      bulk_g2s(dst + seg, rowp + (x0 + tw < g.nx ? x0 + tw : 0), hal, bar);
+    }
+  }
+}
+
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__global__ void __launch_bounds__(128) aa_tma_kernel(const __grid_constant__ AAParams p,
+                                                     typename SP::S* __restrict__ A,
+                                                     const uint8_t* __restrict__ flags) {
+  using S = typename SP::S;
+  using C = typename SP::C;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) unsigned long long bars[TMA_MAX_STAGES];
+  const Grid& g = p.g;
+  const TmaCfg& T = p.tma;
+  const int t = threadIdx.x;
+  const int NS = T.stages;
+  const long long G = gridDim.x;
+  const long long first = blockIdx.x;
+  const long long ntb = first < T.ntiles ? (T.ntiles - first + G - 1) / G : 0;
+  const uint8_t slow_bit = ODD ? 2 : 1;
+  clear_record(p.zero_next);
+  if (t == 0) {
+    for (int s = 0; s < NS; s++) mbar_init(smem_u32(&bars[s]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  uint32_t pending = 0;  // thread 0: stages with loads in flight
+  auto issue = [&](long long k) {
+    if (k >= ntb) return;
+    const long long tile = first + k * G;
+    if (T.tile_slow[tile] & slow_bit) return;
+    const int s = (int)(k % NS);
+    tma_issue<SP, ODD>(p, A, tile, smem + (size_t)s * T.stage_bytes, smem_u32(&bars[s]));
+    pending |= 1u << s;
+  };
+  if (t == 0)
+    for (long long k = 0; k < NS - 1; k++) issue(k);
+  uint32_t phases = 0;
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  bool failed = false;
+  const C rho0 = C(p.rho0);
+  const Coll<C> kc{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
+  for (long long k = 0; k < ntb; k++) {
+    const long long tile = first + k * G;
+    const int s = (int)(k % NS);
+    if (t == 0) issue(k + NS - 1);
+    const long long row = tile / T.ntx;
+    const int x0 = (int)(tile - row * T.ntx) * T.tw;
+    const int y = (int)(row % g.ny), z = (int)(row / g.ny);
+    const int x = x0 + t;
+    if (T.tile_slow[tile] & slow_bit) {
+      aa_direct<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, true, acc, &has_link);
+      continue;
+    }
+    const bool ok = mbar_wait(smem_u32(&bars[s]), (phases >> s) & 1u);
+    phases ^= 1u << s;
+    const S* st = (const S*)(smem + (size_t)s * T.stage_bytes);
+    C f[Q];
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      int idx = t;
+      if (ODD) idx = cx(d) == 1 ? T.halo - 1 + t : (cx(d) == -1 ? t + 1 : t);
+      f[d] = SP::ld(st + d * T.buf_elems + idx, d, rho0);
+    }
+    if (t == 0) pending &= ~(1u << s);
+    if (!__syncthreads_and(ok)) {  // stage consumed (or a wait gave up everywhere)
+      failed = true;
+      break;
+    }
+    C rho, ux, uy, uz;
+    moments<C, FORCE>(f, kc, rho, ux, uy, uz);
+    C pst[Q];
+    collide<C, TRT, FORCE>(f, pst, kc, rho, ux, uy, uz);
+    const long long i = row * g.nx + x;
+    S* const base = A + i;
+    long long fix_lo = 0, fix_hi = 0;
+    if (ODD) {
+      fix_lo = x == 0 ? (long long)g.nx : 0;
+      fix_hi = x == g.nx - 1 ? (long long)g.nx : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+      long long o = p.off_wr[j];
+      if (ODD) {
+        if (cx(j) == 1) o -= fix_hi;
+        if (cx(j) == -1) o += fix_lo;
+      }
+      SP::st(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
+    }
+  }
+  if (failed) {
+    if (t == 0) {
+      atomicExch(T.err, 1);
+      // drain the copies this block still has in flight (bounded)
+      for (int s = 0; s < NS; s++)
+        if (pending & (1u << s)) mbar_wait(smem_u32(&bars[s]), (phases >> s) & 1u);
+    }
+    __syncthreads();
   }
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
@@ -552,7 +767,52 @@ __global__ void aa_init_kernel(const InitParams p, typename SP::S* __restrict__ 
 template <class SP, bool ODD, bool TRT, bool FORCE>
 static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, dim3 grid, dim3 block,
                               cudaStream_t s) {
+  if (p.tma.enabled) {
+    auto kern = aa_tma_kernel<SP, ODD, TRT, FORCE>;
+    const int smem = p.tma.stages * p.tma.stage_bytes;
+    static thread_local int configured_smem = -1;  // per instantiation
+    if (configured_smem != smem) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      configured_smem = smem;
+    }
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p.tma.tw, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    long long nb = (long long)sms * per_sm;
+    if (nb > p.tma.ntiles) nb = p.tma.ntiles;
+    kern<<<(unsigned)nb, p.tma.tw, smem, s>>>(p, (typename SP::S*)A, flags);
+    return cudaGetLastError();
+  }
   aa_step_kernel<SP, ODD, TRT, FORCE><<<grid, block, 0, s>>>(p, (typename SP::S*)A, flags);
+  return cudaGetLastError();
+}
+
+// Per-tile boundary bits: 1 = the even phase needs the direct path, 2 = the odd
+// phase does (boundary node in the tile, or a y/z-periodic wrap row).
+__global__ void tile_flags_kernel(const Grid g, int tw, long long ntiles, const uint8_t* __restrict__ flags,
+                                  uint8_t* __restrict__ tiles) {
+  const long long tile = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tile >= ntiles) return;
+  const long long ntx = g.nx / tw;
+  const long long row = tile / ntx;
+  const int x0 = (int)(tile - row * ntx) * tw;
+  const int y = (int)(row % g.ny), z = (int)(row / g.ny);
+  bool face = (!g.per[1] && (y == 0 || y == g.ny - 1)) || (!g.per[2] && (z == 0 || z == g.nz - 1)) ||
+              (!g.per[0] && (x0 == 0 || x0 + tw == g.nx));
+  bool bnd = face;
+  const uint8_t* f = flags + row * g.nx + x0;
+  for (int k = 0; k < tw && !bnd; k++) bnd = (f[k] & (F_SOLID | F_SOLID_PREV | F_NEAR)) != 0;
+  const bool wrap_row = y == 0 || y == g.ny - 1 || z == 0 || z == g.nz - 1;
+  tiles[tile] = (uint8_t)((bnd ? 1 : 0) | ((bnd || wrap_row) ? 2 : 0));
+}
+
+cudaError_t aa_launch_tile_flags(const Grid& g, int tw, long long ntiles, const uint8_t* flags, uint8_t* tiles,
+                                 cudaStream_t s) {
+  tile_flags_kernel<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(g, tw, ntiles, flags, tiles);
   return cudaGetLastError();
 }
 

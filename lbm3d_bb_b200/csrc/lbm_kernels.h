@@ -5,6 +5,20 @@
 
 namespace lbm {
 
+// TMA-staged persistent variant of the config-mode step.
+struct TmaCfg {
+  int enabled;
+  int tw;          // tile width (cells along x), = block size
+  int halo;        // elements in a 16-byte halo chunk
+  int ntx;         // tiles per row
+  long long ntiles;
+  int stages;      // pipeline depth
+  int stage_bytes; // shared memory per stage (19 direction buffers)
+  int buf_elems;   // elements per direction buffer (tw + halo)
+  const uint8_t* tile_slow;  // per tile: bit 0 even / bit 1 odd phase needs the direct path
+  int* err;                  // set to 1 when a pipeline wait gives up
+};
+
 // Config-mode (AA) step.
 struct AAParams {
   Grid g;
@@ -20,6 +34,7 @@ struct AAParams {
   // the 19 writes of this phase (even: own slots; odd: neighbour slots)
   long long off_rd[19];
   long long off_wr[19];
+  TmaCfg tma;
 };
 
 // Reference-mode step (two population buffers, virtual-fluid solids).
@@ -165,6 +180,8 @@ cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, co
                              const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
                              double* out, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t aa_launch_tile_flags(const Grid& g, int tw, long long ntiles, const uint8_t* flags, uint8_t* tiles,
+                                 cudaStream_t s);
 cudaError_t aa_launch_init(int storage, const InitParams& p, void* A, const uint8_t* flags, dim3 grid,
                            dim3 block, cudaStream_t s);
 
