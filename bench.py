@@ -265,6 +265,7 @@ def roofline(storage, ms_per_launch, n_cells, n_solid, peak, peak_kind, traffic)
 
 
 def main():
+    global GX
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -275,8 +276,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--gx", type=float, default=GX, help="body acceleration along x (workload default 1e-6)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    GX = args.gx
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -183,8 +183,12 @@ __global__ void moving_kernel(const __grid_constant__ FlagParams p, uint8_t* fla
 
 // NEAR: the node is fluid in either flag set and (it was uncovered, or a
 // neighbour is solid in either set).  Reference mode ignores the periodic wrap,
-// as nbr_lli does (Utilities.jl:559-569).
-__global__ void near_kernel(const Grid g, int mode, const Box box, uint8_t* flags) {
+// as nbr_lli does (Utilities.jl:559-569).  Config mode also stores, per node, the
+// link word used by the step kernel: bit d (0..17) = the source x - c_d of incoming
+// direction d is solid now, bit 18+d = it was solid at the last step, bit 36+d =
+// it belongs to the moving body now (sources outside a non-periodic face: no bit).
+__global__ void near_kernel(const Grid g, int mode, const Box box, uint8_t* flags,
+                            unsigned long long* links) {
   const int bx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ex = box.hi[0] - box.lo[0] + 1;
   if (bx >= ex) return;
@@ -194,29 +198,33 @@ __global__ void near_kernel(const Grid g, int mode, const Box box, uint8_t* flag
   const long long i = node_index(g, x, y, z);
   const uint8_t fl = flags[i];
   const bool sc = fl & F_SOLID, sp = fl & F_SOLID_PREV;
-  bool near = false;
-  if (!sc || !sp) {
-    near = sp && !sc;
-    const bool wrap = (mode == LBM_MODE_CONFIG);
+  const bool wrap = (mode == LBM_MODE_CONFIG);
+  bool near = sp && !sc;
+  unsigned long long lw = 0;
 #pragma unroll
-    for (int d = 0; d < 18; d++) {
-      int nx_ = x + cx(d), ny_ = y + cy(d), nz_ = z + cz(d);
-      if (nx_ < 0 || nx_ >= g.nx) {
-        if (!(wrap && g.per[0])) continue;
-        nx_ = wrapc(nx_, g.nx);
-      }
-      if (ny_ < 0 || ny_ >= g.ny) {
-        if (!(wrap && g.per[1])) continue;
-        ny_ = wrapc(ny_, g.ny);
-      }
-      if (nz_ < 0 || nz_ >= g.nz) {
-        if (!(wrap && g.per[2])) continue;
-        nz_ = wrapc(nz_, g.nz);
-      }
-      if (flags[node_index(g, nx_, ny_, nz_)] & (F_SOLID | F_SOLID_PREV)) near = true;
+  for (int d = 0; d < 18; d++) {
+    int nx_ = x - cx(d), ny_ = y - cy(d), nz_ = z - cz(d);
+    if (nx_ < 0 || nx_ >= g.nx) {
+      if (!(wrap && g.per[0])) continue;
+      nx_ = wrapc(nx_, g.nx);
     }
+    if (ny_ < 0 || ny_ >= g.ny) {
+      if (!(wrap && g.per[1])) continue;
+      ny_ = wrapc(ny_, g.ny);
+    }
+    if (nz_ < 0 || nz_ >= g.nz) {
+      if (!(wrap && g.per[2])) continue;
+      nz_ = wrapc(nz_, g.nz);
+    }
+    const uint8_t fn = flags[node_index(g, nx_, ny_, nz_)];
+    if (fn & (F_SOLID | F_SOLID_PREV)) near = true;
+    if (fn & F_SOLID) lw |= 1ull << d;
+    if (fn & F_SOLID_PREV) lw |= 1ull << (18 + d);
+    if (fn & F_MOVING) lw |= 1ull << (36 + d);
   }
+  near = near && (!sc || !sp);
   flags[i] = near ? (uint8_t)(fl | F_NEAR) : (uint8_t)(fl & ~F_NEAR);
+  if (links) links[i] = lw;
 }
 
 // ---- link CSR ----------------------------------------------------------------------------------
@@ -385,8 +393,9 @@ cudaError_t geo_launch_moving(const FlagParams& p, uint8_t* flags, cudaStream_t 
   return cudaGetLastError();
 }
 
-cudaError_t geo_launch_near(const Grid& g, int mode, const Box& box, uint8_t* flags, cudaStream_t s) {
-  near_kernel<<<box_grid(box, 128), 128, 0, s>>>(g, mode, box, flags);
+cudaError_t geo_launch_near(const Grid& g, int mode, const Box& box, uint8_t* flags, unsigned long long* links,
+                            cudaStream_t s) {
+  near_kernel<<<box_grid(box, 128), 128, 0, s>>>(g, mode, box, flags, links);
   return cudaGetLastError();
 }
 

@@ -390,22 +390,26 @@ __device__ __noinline__ void aa_general(const AAParams& p, typename SP::S* __res
   *has_out = *has_out || has_link;
 }
 
-// Interior fast path: no boundary in reach, neighbour offsets precomputed on the
-// host (p.off_rd / p.off_wr); only the periodic x wrap is patched per lane.
-template <class SP, bool ODD, bool TRT, bool FORCE>
-__device__ __forceinline__ void aa_fast(const AAParams& p, typename SP::S* __restrict__ A, const long long i,
-                                        const int x) {
-  using S = typename SP::S;
+// Fast path: interior node whose only boundaries are static no-slip links (bc =
+// incoming directions whose source is solid; 0 for most nodes).  Neighbour offsets
+// are precomputed on the host (p.off_rd / p.off_wr); the periodic x wrap is patched
+// per lane.  A static no-slip bounce-back value for incoming d is f*_{opp(d)}: in
+// the even phase that is exactly the swapped store, in the odd phase it only
+// redirects the store of f*_j from the solid target x + c_j to the own slot opp(j).
+//
+// The loads are split from the compute so that the caller can issue them before the
+// node's flag byte arrives (speculatively, for every lane whose coordinates allow
+// the fast path), instead of chaining two memory round trips.
+template <class SP, bool ODD>
+__device__ __forceinline__ void aa_fast_load(const AAParams& p, const typename SP::S* __restrict__ base,
+                                             const int x, typename SP::C* f) {
   using C = typename SP::C;
   const C rho0 = C(p.rho0);
-  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
-  S* const base = A + i;
   long long fix_lo = 0, fix_hi = 0;  // periodic x wrap at the row ends (odd phase)
   if (ODD) {
     fix_lo = x == 0 ? (long long)p.g.nx : 0;
     fix_hi = x == p.g.nx - 1 ? (long long)p.g.nx : 0;
   }
-  C f[Q];
 #pragma unroll
   for (int d = 0; d < Q; d++) {
     long long o = p.off_rd[d];
@@ -414,6 +418,25 @@ __device__ __forceinline__ void aa_fast(const AAParams& p, typename SP::S* __res
       if (cx(d) == -1) o -= fix_hi;
     }
     f[d] = SP::ld(base + o, d, rho0);
+  }
+}
+
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S* __restrict__ base,
+                                               const int x, const int y, const int z, const uint32_t bc,
+                                               typename SP::C* f, double* acc, bool* has_link) {
+  using C = typename SP::C;
+  const C rho0 = C(p.rho0);
+  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
+  if (ODD && bc) {  // bounce-back values are kept in the own slots
+#pragma unroll
+    for (int d = 0; d < 18; d++)
+      if ((bc >> d) & 1u) f[d] = SP::ld(base + (long long)d * p.g.plane, d, rho0);
+  }
+  long long fix_lo = 0, fix_hi = 0;
+  if (ODD) {
+    fix_lo = x == 0 ? (long long)p.g.nx : 0;
+    fix_hi = x == p.g.nx - 1 ? (long long)p.g.nx : 0;
   }
   C rho, ux, uy, uz;
   moments<C, FORCE>(f, k, rho, ux, uy, uz);
@@ -425,34 +448,69 @@ __device__ __forceinline__ void aa_fast(const AAParams& p, typename SP::S* __res
     if (ODD) {
       if (cx(j) == 1) o -= fix_hi;
       if (cx(j) == -1) o += fix_lo;
+      if (j < 18 && ((bc >> opp(j)) & 1u)) o = (long long)opp(j) * p.g.plane;
     }
     SP::st(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
   }
+  if (bc && p.compute_force) {
+    // momentum exchange of the static links: c_o (f*_o + f*_o), o = opp(d)
+#pragma unroll
+    for (int d = 0; d < 18; d++) {
+      if (!((bc >> d) & 1u)) continue;
+      const int o = opp(d);
+      const double t = 2.0 * (double)pst[o];
+      const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
+      const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
+      const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
+      const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
+      acc[0] += fx;
+      acc[1] += fy;
+      acc[2] += fz;
+      acc[3] += ry * fz - rz * fy;
+      acc[4] += rz * fx - rx * fz;
+      acc[5] += rx * fy - ry * fx;
+    }
+    *has_link = true;
+  }
 }
 
-// One node on the direct path: warps with no boundary in reach take the fast path,
-// others the general path.  Lanes of a warp must belong to the same launch shape
-// (all 32 lanes reach the vote).
+// One node on the direct path: lanes whose coordinates allow the fast path issue
+// their population loads at once; the flag byte (and, next to a solid, the link
+// word) decides afterwards whether the warp finishes on the fast path or reruns the
+// node on the general path.  All 32 lanes of a warp reach the vote.
 template <class SP, bool ODD, bool TRT, bool FORCE>
 __device__ __forceinline__ void aa_direct(const AAParams& p, typename SP::S* __restrict__ A,
                                           const uint8_t* __restrict__ flags, const int x, const int y, const int z,
                                           const bool inb, double* acc, bool* has_link) {
+  using C = typename SP::C;
   const Grid& g = p.g;
   const long long i = inb ? node_index(g, x, y, z) : 0;
-  const uint8_t fl = inb ? flags[i] : (uint8_t)F_SOLID;
-  const bool solid = (fl & F_SOLID) != 0;
-  // A lane may take the fast path when no boundary is in reach: not NEAR, not on a
-  // non-periodic face, and (odd phase) no y/z wrap.
   const bool xin = g.per[0] || (x > 0 && x < g.nx - 1);
-  bool fast = !(fl & F_NEAR) && xin;
+  bool coord_fast = inb && xin;
   if (ODD) {
-    fast = fast && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
+    coord_fast = coord_fast && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
   } else {
-    fast = fast && (g.per[1] || (y > 0 && y < g.ny - 1)) && (g.per[2] || (z > 0 && z < g.nz - 1));
+    coord_fast = coord_fast && (g.per[1] || (y > 0 && y < g.ny - 1)) && (g.per[2] || (z > 0 && z < g.nz - 1));
   }
+  const uint8_t fl = inb ? flags[i] : (uint8_t)F_SOLID;
+  C f[Q];
+  if (coord_fast) aa_fast_load<SP, ODD>(p, A + i, x, f);  // in-bounds: interior in every non-wrapped axis
+  const bool solid = (fl & F_SOLID) != 0;
+  // fast when the only boundaries are static no-slip links (link word: current ==
+  // previous links, no moving-body link, not uncovered)
+  uint32_t bc = 0;
+  bool static_links = true;
+  if (!solid && (fl & F_NEAR)) {
+    const unsigned long long lw = p.links[i];
+    const uint32_t cur = (uint32_t)(lw & 0x3FFFFu), prev = (uint32_t)((lw >> 18) & 0x3FFFFu);
+    const uint32_t mov = (uint32_t)((lw >> 36) & 0x3FFFFu);
+    static_links = cur == prev && mov == 0 && !(fl & F_SOLID_PREV);
+    bc = cur;
+  }
+  const bool fast = coord_fast && static_links;
   const bool warp_fast = __all_sync(0xffffffffu, solid || fast);
   if (warp_fast) {
-    if (!solid) aa_fast<SP, ODD, TRT, FORCE>(p, A, i, x);
+    if (!solid) aa_fast_finish<SP, ODD, TRT, FORCE>(p, A + i, x, y, z, bc, f, acc, has_link);
   } else if (!solid) {
     aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, i, fl, acc, has_link);
   }

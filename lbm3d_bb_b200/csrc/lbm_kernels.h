@@ -35,6 +35,9 @@ struct AAParams {
   long long off_rd[19];
   long long off_wr[19];
   TmaCfg tma;
+  // per-node link words of NEAR nodes (see near_kernel): static no-slip links stay
+  // on the fast path, everything else takes the general path
+  const unsigned long long* links;
 };
 
 // Reference-mode step (two population buffers, virtual-fluid solids).
@@ -218,7 +221,8 @@ cudaError_t geo_launch_static(const Grid& g, const BodyDev& b, const Box& box, u
 cudaError_t geo_launch_spheres(const Grid& g, const double* xyzr, int count, uint8_t* flags,
                                cudaStream_t s);
 cudaError_t geo_launch_moving(const FlagParams& p, uint8_t* flags, cudaStream_t s);
-cudaError_t geo_launch_near(const Grid& g, int mode, const Box& box, uint8_t* flags, cudaStream_t s);
+cudaError_t geo_launch_near(const Grid& g, int mode, const Box& box, uint8_t* flags, unsigned long long* links,
+                            cudaStream_t s);
 cudaError_t geo_launch_sync_prev(const Grid& g, uint8_t* flags, cudaStream_t s);
 // Link export: counts per node (cur solid bits), exclusive scan, CSR fill.
 cudaError_t geo_links(const Grid& g, int mode, const uint8_t* flags, uint8_t solid_bit, int32_t* d_count,

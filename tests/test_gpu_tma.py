@@ -30,15 +30,15 @@ def _porous(cls, storage, nx=128, ny=24, nz=20, steps=9, seed=5, **kw):
 
 
 def _with_tma(enabled: bool, fn):
-    old = os.environ.get("LBM3D_NO_TMA")
-    os.environ["LBM3D_NO_TMA"] = "0" if enabled else "1"
+    old = os.environ.get("LBM3D_TMA")
+    os.environ["LBM3D_TMA"] = "1" if enabled else "0"
     try:
         return fn()
     finally:
         if old is None:
-            del os.environ["LBM3D_NO_TMA"]
+            del os.environ["LBM3D_TMA"]
         else:
-            os.environ["LBM3D_NO_TMA"] = old
+            os.environ["LBM3D_TMA"] = old
 
 
 @pytest.mark.parametrize("storage", ["fp32", "fp16dev", "fp64"])
