@@ -246,6 +246,24 @@ int32_t lbm_get_flags(lbm_ctx* ctx, uint8_t* mask_s, uint8_t* mask_bb);
  * arrays; *nnz is always written.  LBM_ERR_CAPACITY when cap < nnz.  Blocking. */
 int32_t lbm_get_links(lbm_ctx* ctx, int32_t* bb_ptr, int32_t* bb_lidxs, int8_t* bb_dirs,
                       int64_t cap, int64_t* nnz);
+/* Link CSR export that allocates nothing; no counterpart in the reference.
+ * Writes the same CSR as lbm_get_links, bit for bit, into caller-provided DEVICE
+ * arrays: d_bb_ptr[N+1], d_bb_lidxs[cap], d_bb_dirs[cap].  For callers that cannot
+ * call cudaMalloc: a host runtime that owns the device memory pool and must account
+ * for every byte (CUDA.jl's allocator when MainCore.jl drives this library), and loops
+ * that must not pay the device-wide synchronisation that cudaMalloc/cudaFree imply
+ * (the reference rebuilds its link list every step, Motion.jl:82-93).
+ * Its only scratch is a file-scope device array of 131,073 int64 (1 MiB), one entry
+ * per 1024 nodes: every GPU that loads the library holds it until the process exits,
+ * and lattices above 134,217,728 nodes (512^3) are rejected with LBM_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls
+ * share the array and it keeps the last call's contents (each call overwrites every
+ * entry it reads); calls that overlap on the GPU — other streams or host threads —
+ * race on it.  *nnz is always written; LBM_ERR_CAPACITY when cap < nnz (link entries
+ * beyond cap are not written).  Blocking: waits for nnz on the context's stream. */
+int32_t lbm_get_links_noalloc(lbm_ctx* ctx, int32_t* d_bb_ptr, int32_t* d_bb_lidxs, int8_t* d_bb_dirs,
+                              int64_t cap, int64_t* nnz);
 /* FP64 sum of all populations over fluid nodes (reference mode: all nodes).
  * Blocking. */
 int32_t lbm_mass(lbm_ctx* ctx, double* out);

@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
         "lbm_get_populations": (i32, [vp, vp, i32, i32, i32]),
         "lbm_get_flags": (i32, [vp, vp, vp]),
         "lbm_get_links": (i32, [vp, vp, vp, vp, i64, P(i64)]),
+        "lbm_get_links_noalloc": (i32, [vp, vp, vp, vp, i64, P(i64)]),
         "lbm_mass": (i32, [vp, P(f64)]),
         "lbm_check": (i32, [vp]),
     }
@@ -83,7 +84,7 @@ def exported_symbols() -> list[str]:
         "lbm_device_bytes", "lbm_set_launch", "lbm_get_launch", "lbm_add_body", "lbm_add_spheres",
         "lbm_update_body", "lbm_init_equilibrium", "lbm_set_populations", "lbm_step", "lbm_step_count", "lbm_launch_count",
         "lbm_get_force", "lbm_get_force_history", "lbm_get_macros", "lbm_get_populations", "lbm_get_flags",
-        "lbm_get_links", "lbm_mass", "lbm_check",
+        "lbm_get_links", "lbm_get_links_noalloc", "lbm_mass", "lbm_check",
     ]
 
 

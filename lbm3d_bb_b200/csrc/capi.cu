@@ -1101,6 +1101,30 @@ int32_t lbm_get_links(lbm_ctx* c, int32_t* bb_ptr, int32_t* bb_lidxs, int8_t* bb
   return LBM_OK;
 }
 
+int32_t lbm_get_links_noalloc(lbm_ctx* c, int32_t* d_bb_ptr, int32_t* d_bb_lidxs, int8_t* d_bb_dirs, int64_t cap,
+                              int64_t* nnz) {
+  if (!c || !nnz || !d_bb_ptr) return LBM_ERR_ARG;
+  if (cap > 0 && (!d_bb_lidxs || !d_bb_dirs)) return c->fail(LBM_ERR_ARG, "null link arrays with cap > 0");
+  if (c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  if (c->g.N > geo_links_noalloc_max_nodes())
+    return c->fail(LBM_ERR_CAPACITY, "lbm_get_links_noalloc supports at most %lld nodes (lattice has %lld)",
+                   geo_links_noalloc_max_nodes(), c->g.N);
+  int rc = sync_flags(c);
+  if (rc) return rc;
+  long long total = 0;
+  int too_large = 0;
+  if (c->cuda(geo_links_noalloc(c->g, c->cfg.mode, c->flags, F_SOLID, d_bb_ptr, d_bb_lidxs, d_bb_dirs,
+                                std::max<long long>(cap, 0), &total, &too_large, c->stream),
+              "links (no allocation)"))
+    return LBM_ERR_CUDA;
+  if (too_large)
+    return c->fail(LBM_ERR_CAPACITY, "lbm_get_links_noalloc supports at most %lld nodes", geo_links_noalloc_max_nodes());
+  *nnz = total;
+  if (total >= (1LL << 31) - 1) return c->fail(LBM_ERR_CAPACITY, "more than 2^31-2 links do not fit the Int32 CSR");
+  if (total > cap) return c->fail(LBM_ERR_CAPACITY, "link capacity %lld < nnz %lld", (long long)cap, total);
+  return LBM_OK;
+}
+
 int32_t lbm_mass(lbm_ctx* c, double* out) {
   if (!c || !out) return LBM_ERR_ARG;
   if (!c->initialised) return c->fail(LBM_ERR_STATE, "not initialised");

@@ -9,6 +9,8 @@
 //
 // Compiled with --fmad=false: every predicate rounds as written, exactly like the
 // CPU restatement built with -ffp-contract=off, so flags and links are bit-exact.
+#include <mutex>
+
 #include "lbm_internal.cuh"
 #include "lbm_kernels.h"
 
@@ -428,5 +430,101 @@ cudaError_t geo_masks(const Grid& g, int mode, const uint8_t* flags, uint8_t sbi
   masks_kernel<<<(unsigned)((g.N + 255) / 256), 256, 0, s>>>(g, mode, flags, sbit, ms, mb);
   return cudaGetLastError();
 }
+
+// ---- link CSR without allocation -----------------------------------------------------
+// Same CSR as geo_links, for callers that cannot allocate device memory.  The only
+// scratch is one int64 per 1024-node block (the block's link count, then its
+// exclusive offset), kept in this file-scope array; per-node offsets are recomputed
+// from the flags in the fill pass instead of being stored.  The array lives on every
+// device that loads the library until the process exits, holds the last call's
+// contents between calls, and is shared by all calls: calls that overlap on the GPU
+// race on it.
+constexpr long long NOALLOC_MAX_BLOCKS = 131072;  // 131072 * 1024 = 134,217,728 nodes (512^3)
+static __device__ __align__(256) long long g_noalloc_block_sums[NOALLOC_MAX_BLOCKS + 1];
+
+__global__ void na_count_kernel(const Grid g, int mode, const uint8_t* __restrict__ flags, uint8_t sbit,
+                                long long* __restrict__ bs) {
+  const long long i = (long long)blockIdx.x * SCAN_B + threadIdx.x;
+  long long v = 0;
+  if (i < g.N) {
+    const int x = (int)(i % g.nx);
+    const int y = (int)((i / g.nx) % g.ny);
+    const int z = (int)(i / ((long long)g.nx * g.ny));
+    v = __popc(link_mask(g, mode, flags, sbit, x, y, z));
+  }
+  long long total;
+  block_exclusive_scan(v, &total);
+  if (threadIdx.x == 0) bs[blockIdx.x] = total;  // every block of this call overwrites its entry
+}
+
+__global__ void na_fill_kernel(const Grid g, int mode, const uint8_t* __restrict__ flags, uint8_t sbit,
+                               const long long* __restrict__ bs, long long nb, int32_t* __restrict__ ptr,
+                               int32_t* __restrict__ lidx, int8_t* __restrict__ dirs, long long cap) {
+  const long long i = (long long)blockIdx.x * SCAN_B + threadIdx.x;
+  uint32_t m = 0;
+  if (i < g.N) {
+    const int x = (int)(i % g.nx);
+    const int y = (int)((i / g.nx) % g.ny);
+    const int z = (int)(i / ((long long)g.nx * g.ny));
+    m = link_mask(g, mode, flags, sbit, x, y, z);
+  }
+  const long long ex = block_exclusive_scan((long long)__popc(m), nullptr) + bs[blockIdx.x];
+  if (i < g.N) {
+    ptr[i] = (int32_t)(1 + ex);
+    long long k = ex;
+    for (int d = 0; d < 18; d++) {
+      if ((m >> d) & 1u) {
+        if (k < cap) {  // never write past the caller's capacity
+          lidx[k] = (int32_t)(i + 1);
+          dirs[k] = (int8_t)(d + 1);
+        }
+        k++;
+      }
+    }
+  }
+  if (i == 0) ptr[g.N] = (int32_t)(1 + bs[nb]);
+}
+
+namespace {
+// Device address of g_noalloc_block_sums per device.  Host code must not use the
+// array's name as a device pointer: it is a host-side stand-in.
+constexpr int NOALLOC_MAX_DEVICES = 64;
+long long* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+std::mutex g_noalloc_mutex;
+}  // namespace
+
+cudaError_t geo_links_noalloc(const Grid& g, int mode, const uint8_t* flags, uint8_t sbit, int32_t* d_ptr,
+                              int32_t* d_lidx, int8_t* d_dirs, long long cap, long long* h_nnz, int* too_large,
+                              cudaStream_t s) {
+  const long long nb = (g.N + SCAN_B - 1) / SCAN_B;
+  *too_large = nb > NOALLOC_MAX_BLOCKS ? 1 : 0;
+  if (*too_large) return cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+  long long* bs = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {  // once per device, with that device current
+      void* ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, g_noalloc_block_sums);
+      if (e != cudaSuccess) return e;
+      g_noalloc_ptr[dev] = (long long*)ptr;
+    }
+    bs = g_noalloc_ptr[dev];
+  }
+  na_count_kernel<<<(unsigned)nb, SCAN_B, 0, s>>>(g, mode, flags, sbit, bs);
+  scan_blocksums_kernel<<<1, SCAN_B, 0, s>>>(bs, nb);
+  na_fill_kernel<<<(unsigned)nb, SCAN_B, 0, s>>>(g, mode, flags, sbit, bs, nb, d_ptr, d_lidx, d_dirs,
+                                                 d_lidx && d_dirs ? cap : 0);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(h_nnz, bs + nb, sizeof(long long), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);
+}
+
+long long geo_links_noalloc_max_nodes() { return NOALLOC_MAX_BLOCKS * SCAN_B; }
 
 }  // namespace lbm

@@ -228,6 +228,12 @@ cudaError_t geo_launch_sync_prev(const Grid& g, uint8_t* flags, cudaStream_t s);
 cudaError_t geo_links(const Grid& g, int mode, const uint8_t* flags, uint8_t solid_bit, int32_t* d_count,
                       long long* d_scan, long long* d_blocksums, int32_t* d_ptr, int32_t* d_lidx,
                       int8_t* d_dirs, long long cap, long long* h_nnz, cudaStream_t s);
+// Link CSR into caller device arrays with no allocation (file-scope scratch); sets
+// *too_large when the lattice exceeds geo_links_noalloc_max_nodes() and does nothing.
+cudaError_t geo_links_noalloc(const Grid& g, int mode, const uint8_t* flags, uint8_t sbit, int32_t* d_ptr,
+                              int32_t* d_lidx, int8_t* d_dirs, long long cap, long long* h_nnz, int* too_large,
+                              cudaStream_t s);
+long long geo_links_noalloc_max_nodes();
 cudaError_t geo_masks(const Grid& g, int mode, const uint8_t* flags, uint8_t solid_bit, uint8_t* ms,
                       uint8_t* mb, cudaStream_t s);
 
