@@ -62,7 +62,10 @@ enum {
   LBM_FACE_PERIODIC = 0,
   LBM_FACE_WALL = 1,     /* half-way bounce-back, wall velocity face_u[f] (0: no-slip) */
   LBM_FACE_EQ_INLET = 2, /* unknown populations set to feq(rho_node, face_u[f]) */
-  LBM_FACE_OUTFLOW = 3   /* zero-gradient: unknown population = same node's post-collision value */
+  LBM_FACE_OUTFLOW = 3,  /* zero-gradient: unknown population = same node's post-collision value */
+  LBM_FACE_PRESSURE = 4  /* pressure outlet: anti-bounce-back at rho0 with the node's velocity
+                            (the outlet rule of velocity_BC!_gpu, OtherBC.jl:153-166, with the
+                            density fixed to rho0 instead of the node's) */
 };
 
 /* Body kinds. CYLINDER_Z and NACA_Z are the reference's extruded shapes
@@ -269,6 +272,36 @@ int32_t lbm_get_links_noalloc(lbm_ctx* ctx, int32_t* d_bb_ptr, int32_t* d_bb_lid
 int32_t lbm_mass(lbm_ctx* ctx, double* out);
 /* Scans the populations for NaN/Inf; LBM_ERR_NUMERIC when any is found.  Blocking. */
 int32_t lbm_check(lbm_ctx* ctx);
+
+/* ---- batched sweeps ------------------------------------------------------------- */
+/* Many independent config-mode domains of uneven sizes stepped together: every step
+ * is ONE persistent launch over a per-domain work table (runs of 128 cells of one
+ * domain per work item), followed by a one-thread kernel that advances a device step
+ * counter, so a sequence of steps can be captured once in a CUDA graph and replayed.
+ * No reference counterpart: the reference runs one domain per process (MainCore.jl).
+ *
+ * Members: initialised contexts on one device and one stream, all with the same
+ * storage and collision, static bodies only (no moving body).  They keep their own
+ * populations, flags and force rings; lbm_get_force / lbm_get_macros /
+ * lbm_get_populations on a member read the batched result.  A member may still be
+ * stepped alone with lbm_step between batch calls (the table follows it); the batch
+ * must be destroyed before any of its members.  Calls are ordered on the members'
+ * stream. */
+typedef struct lbm_batch lbm_batch;
+int32_t lbm_batch_create(lbm_ctx* const* ctxs, int32_t count, lbm_batch** out);
+int32_t lbm_batch_destroy(lbm_batch* b);
+const char* lbm_batch_last_error(const lbm_batch* b);
+/* `nsteps` batched steps, enqueued as 2 launches per step. */
+int32_t lbm_batch_step(lbm_batch* b, int32_t nsteps);
+/* Records `nsteps` batched steps into a CUDA graph (replacing an earlier one); runs
+ * nothing.  The capture uses a private stream. */
+int32_t lbm_batch_capture(lbm_batch* b, int32_t nsteps);
+/* Launches the captured graph `times` times on the members' stream. */
+int32_t lbm_batch_replay(lbm_batch* b, int32_t times);
+/* Kernels the batch has launched, graph nodes included. */
+int64_t lbm_batch_launch_count(const lbm_batch* b);
+/* Waits for the members' stream; LBM_ERR_CUDA with the CUDA error otherwise. */
+int32_t lbm_batch_synchronize(lbm_batch* b);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,14 @@ def lib() -> C.CDLL:
         "lbm_get_links_noalloc": (i32, [vp, vp, vp, vp, i64, P(i64)]),
         "lbm_mass": (i32, [vp, P(f64)]),
         "lbm_check": (i32, [vp]),
+        "lbm_batch_create": (i32, [vp, i32, P(vp)]),
+        "lbm_batch_destroy": (i32, [vp]),
+        "lbm_batch_last_error": (C.c_char_p, [vp]),
+        "lbm_batch_step": (i32, [vp, i32]),
+        "lbm_batch_capture": (i32, [vp, i32]),
+        "lbm_batch_replay": (i32, [vp, i32]),
+        "lbm_batch_launch_count": (i64, [vp]),
+        "lbm_batch_synchronize": (i32, [vp]),
     }
     for name, (res, args) in proto.items():
         fn = getattr(L, name)
@@ -85,6 +93,8 @@ def exported_symbols() -> list[str]:
         "lbm_update_body", "lbm_init_equilibrium", "lbm_set_populations", "lbm_step", "lbm_step_count", "lbm_launch_count",
         "lbm_get_force", "lbm_get_force_history", "lbm_get_macros", "lbm_get_populations", "lbm_get_flags",
         "lbm_get_links", "lbm_get_links_noalloc", "lbm_mass", "lbm_check",
+        "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_last_error", "lbm_batch_step", "lbm_batch_capture",
+        "lbm_batch_replay", "lbm_batch_launch_count", "lbm_batch_synchronize",
     ]
 
 

@@ -30,6 +30,7 @@ FACE_PERIODIC = 0
 FACE_WALL = 1
 FACE_EQ_INLET = 2
 FACE_OUTFLOW = 3
+FACE_PRESSURE = 4
 
 BODY_CYLINDER_Z = 1
 BODY_NACA_Z = 2
@@ -45,7 +46,8 @@ DEVICE = 1
 
 STORAGE = {"fp32": STORE_FP32, "fp64": STORE_FP64, "fp16dev": STORE_FP16DEV}
 COLLISION = {"BGK": COLL_BGK, "TRT": COLL_TRT}
-FACES = {"periodic": FACE_PERIODIC, "wall": FACE_WALL, "inlet": FACE_EQ_INLET, "outflow": FACE_OUTFLOW}
+FACES = {"periodic": FACE_PERIODIC, "wall": FACE_WALL, "inlet": FACE_EQ_INLET, "outflow": FACE_OUTFLOW,
+         "pressure": FACE_PRESSURE}
 
 
 class LbmConfig(C.Structure):

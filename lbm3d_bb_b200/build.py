@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -24,6 +25,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 # per-file flags: exact rounding (no FMA contraction) where bit-exact parity is required
 PER_FILE = {
     "kernels_aa.cu": [],
+    "kernels_aa_fp32.cu": [],
+    "kernels_aa_fp64.cu": [],
+    "kernels_aa_fp16.cu": [],
     "kernels_ref.cu": ["--fmad=false"],
     "geometry.cu": ["--fmad=false"],
     "capi.cu": [],
@@ -48,7 +52,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     """Compiles every CUDA source for sm_100a and links liblbm3d.so; returns its path."""
     OBJ.mkdir(exist_ok=True)
     headers = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "lbm3d.h"]
-    objs = []
+    objs, jobs = [], []
     for src, flags in PER_FILE.items():
         s = CSRC / src
         o = OBJ / (s.stem + ".o")
@@ -58,7 +62,13 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            jobs.append(cmd)
+    # translation units compile independently: run them side by side
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=not verbose, text=True), jobs):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed ({r.returncode}): {' '.join(r.args)}\n{r.stderr or ''}")
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
         if verbose:

@@ -98,10 +98,16 @@ struct lbm_ctx {
 namespace {
 
 void default_block(lbm_ctx* c) {
-  int nx = c->g.nx;
+  // rows of the box across threadIdx.x; whole warps, at most 256 threads (the step
+  // kernels' launch bound).  Rows that fit no such shape are padded to 32 lanes.
+  const int nx = c->g.nx;
   int bx = nx <= 128 ? nx : 128;
   int by = std::max(1, 128 / bx);
-  while ((bx * by) % 32 != 0) by++;
+  while ((bx * by) % 32 != 0 && bx * (by + 1) <= 256) by++;
+  if ((bx * by) % 32 != 0) {
+    bx = (nx + 31) / 32 * 32;
+    by = std::max(1, 128 / bx);
+  }
   const char* env = std::getenv("LBM3D_BLOCK");
   if (env) {
     int ex = 0, ey = 0;
@@ -362,6 +368,40 @@ int reduce_state(lbm_ctx* c, double out[2]) {
   return LBM_OK;
 }
 
+// Parameter block of the config-mode step for one phase (odd: the populations are in
+// the swapped layout).  force/zero_next are left for the caller.
+void fill_aa_params(const lbm_ctx* c, AAParams& p, bool odd) {
+  p = AAParams{};
+  p.g = c->g;
+  for (int f = 0; f < 6; f++) {
+    p.face_kind[f] = c->cfg.face[f];
+    for (int a = 0; a < 3; a++) p.face_u[f][a] = c->cfg.face_u[f][a];
+  }
+  p.omega_p = c->cfg.omega_p;
+  p.omega_m = c->cfg.omega_m;
+  p.rho0 = c->cfg.rho0;
+  for (int a = 0; a < 3; a++) p.gacc[a] = c->cfg.accel[a];
+  p.kin = c->kin_latest;
+  if (!c->has_moving)
+    for (int a = 0; a < 3; a++) p.kin.center[a] = c->torque_center[a];
+  p.compute_force = c->cfg.compute_force ? 1 : 0;
+  p.links = c->links;
+  const long long nx = c->g.nx, nxy = (long long)c->g.nx * c->g.ny, pl = c->g.plane;
+  for (int d = 0; d < 19; d++) {
+    const long long nb = cx(d) + nx * cy(d) + nxy * cz(d);
+    if (!odd) {  // even phase: own slots
+      p.off_rd[d] = d * pl;
+      p.off_wr[d] = d * pl;
+    } else {  // odd phase: pull from x - c_d (slot opp(d)), push to x + c_d (slot d)
+      p.off_rd[d] = opp(d) * pl - nb;
+      p.off_wr[d] = d * pl + nb;
+    }
+  }
+}
+
+bool has_force(const lbm_ctx* c) { return c->cfg.accel[0] != 0.0 || c->cfg.accel[1] != 0.0 || c->cfg.accel[2] != 0.0; }
+bool has_faces(const lbm_ctx* c) { return !(c->g.per[0] && c->g.per[1] && c->g.per[2]); }
+
 int near_full(lbm_ctx* c) {
   c->tiles_dirty = true;
   Box f = full_box(c);
@@ -572,7 +612,7 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
       const bool p0 = cfg->face[2 * a] == LBM_FACE_PERIODIC, p1 = cfg->face[2 * a + 1] == LBM_FACE_PERIODIC;
       if (p0 != p1) return set_global(LBM_ERR_ARG, "axis %d: both faces periodic or neither", a);
       for (int s = 0; s < 2; s++)
-        if (cfg->face[2 * a + s] < LBM_FACE_PERIODIC || cfg->face[2 * a + s] > LBM_FACE_OUTFLOW)
+        if (cfg->face[2 * a + s] < LBM_FACE_PERIODIC || cfg->face[2 * a + s] > LBM_FACE_PRESSURE)
           return set_global(LBM_ERR_ARG, "bad face kind");
     }
   }
@@ -889,35 +929,9 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
       c->ref_direct = false;
     } else {
       AAParams p{};
-      p.g = c->g;
-      for (int f = 0; f < 6; f++) {
-        p.face_kind[f] = c->cfg.face[f];
-        for (int a = 0; a < 3; a++) p.face_u[f][a] = c->cfg.face_u[f][a];
-      }
-      p.omega_p = c->cfg.omega_p;
-      p.omega_m = c->cfg.omega_m;
-      p.rho0 = c->cfg.rho0;
-      for (int a = 0; a < 3; a++) p.gacc[a] = c->cfg.accel[a];
-      p.kin = c->kin_latest;
-      if (!c->has_moving)
-        for (int a = 0; a < 3; a++) p.kin.center[a] = c->torque_center[a];
-      p.compute_force = c->cfg.compute_force ? 1 : 0;
+      fill_aa_params(c, p, c->swapped);
       p.force = slot;
       p.zero_next = next;
-      p.links = c->links;
-      {
-        const long long nx = c->g.nx, nxy = (long long)c->g.nx * c->g.ny, pl = c->g.plane;
-        for (int d = 0; d < 19; d++) {
-          const long long nb = cx(d) + nx * cy(d) + nxy * cz(d);
-          if (!c->swapped) {  // even phase: own slots
-            p.off_rd[d] = d * pl;
-            p.off_wr[d] = d * pl;
-          } else {  // odd phase: pull from x - c_d (slot opp(d)), push to x + c_d (slot d)
-            p.off_rd[d] = opp(d) * pl - nb;
-            p.off_wr[d] = d * pl + nb;
-          }
-        }
-      }
       if (c->tma) {
         if (c->tiles_dirty) {
           c->launches++;
@@ -937,10 +951,9 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
         T.tile_slow = c->tiles;
         T.err = c->d_err;
       }
-      const bool force = c->cfg.accel[0] != 0.0 || c->cfg.accel[1] != 0.0 || c->cfg.accel[2] != 0.0;
       c->launches++;
-      rc = c->cuda(aa_launch_step(c->cfg.storage, p, c->A, c->flags, c->swapped, trt, force, c->grid(), c->block(),
-                                  c->stream),
+      rc = c->cuda(aa_launch_step(c->cfg.storage, p, c->A, c->flags, c->swapped, trt, has_force(c), has_faces(c),
+                                  c->grid(), c->block(), c->stream),
                    "AA step");
       if (rc) return rc;
       c->swapped = !c->swapped;
@@ -1145,6 +1158,275 @@ int32_t lbm_check(lbm_ctx* c) {
   if (rc) return rc;
   if (r[1] != 0.0) return c->fail(LBM_ERR_NUMERIC, "%.0f nodes hold non-finite populations", r[1]);
   return pipeline_status(c);
+}
+
+}  // extern "C"
+
+// ---- batched sweeps -------------------------------------------------------------------
+struct lbm_batch {
+  std::vector<lbm_ctx*> ctxs;
+  std::vector<BatchDom> host;  // table as last uploaded
+  int device = 0;
+  int storage = 0;
+  bool trt = false, force = false, faces = false;
+  cudaStream_t stream = nullptr;      // the members' stream
+  cudaStream_t cap_stream = nullptr;  // private stream for graph capture
+  BatchDom* d_doms = nullptr;
+  int* d_item_dom = nullptr;
+  long long* d_counter = nullptr;
+  long long items = 0;
+  long long k_host = 0;  // batch steps enqueued so far (= device counter once they ran)
+  int blocks = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_steps = 0;
+  long long launches = 0;
+  std::string err;
+
+  int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+  }
+  int cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return LBM_OK;
+    return fail(LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+};
+
+namespace {
+
+// Table entry of member m for batch step k_host: the domain has completed
+// ctx->nstep steps and its populations are in the `swapped` layout.
+void batch_entry(const lbm_batch* b, int m, BatchDom& e) {
+  const lbm_ctx* c = b->ctxs[m];
+  const long long item_begin = e.item_begin;
+  e = BatchDom{};
+  fill_aa_params(c, e.p[0], false);
+  fill_aa_params(c, e.p[1], true);
+  e.A = c->A;
+  e.flags = c->flags;
+  e.ring = c->ring;
+  e.ring_slots = c->ring_slots;
+  e.base_step = c->nstep - b->k_host;
+  e.phase0 = (int)(((c->swapped ? 1 : 0) - (b->k_host & 1) + 2) & 1);
+  e.item_begin = item_begin;
+}
+
+// Brings the device table in line with the members (a member stepped alone since the
+// last batch call) and orders the batch after work on the members' stream.
+int batch_refresh(lbm_batch* b) {
+  bool dirty = false;
+  for (size_t m = 0; m < b->ctxs.size(); m++) {
+    const lbm_ctx* c = b->ctxs[m];
+    const BatchDom& e = b->host[m];
+    const bool swapped = ((e.phase0 + b->k_host) & 1) != 0;
+    if (e.base_step + b->k_host != c->nstep || swapped != c->swapped) {
+      batch_entry(b, (int)m, b->host[m]);
+      dirty = true;
+    }
+  }
+  if (dirty &&
+      b->cuda(cudaMemcpyAsync(b->d_doms, b->host.data(), b->host.size() * sizeof(BatchDom), cudaMemcpyHostToDevice,
+                              b->stream),
+              "upload batch table"))
+    return LBM_ERR_CUDA;
+  // pageable source: the copy is staged before cudaMemcpyAsync returns
+  return LBM_OK;
+}
+
+void batch_advance_members(lbm_batch* b, long long n) {
+  b->k_host += n;
+  for (lbm_ctx* c : b->ctxs) {
+    c->nstep += n;
+    if (n & 1) c->swapped = !c->swapped;
+    c->pose_last_step = c->pose_latest;
+    c->kin_last_step = c->kin_latest;
+  }
+}
+
+int batch_enqueue(lbm_batch* b, int nsteps, cudaStream_t s) {
+  BatchParams bp{};
+  bp.doms = b->d_doms;
+  bp.item_dom = b->d_item_dom;
+  bp.items = b->items;
+  bp.counter = b->d_counter;
+  for (int k = 0; k < nsteps; k++) {
+    if (b->cuda(aa_launch_batch(b->storage, bp, b->trt, b->force, b->faces, b->blocks, s), "batched step"))
+      return LBM_ERR_CUDA;
+    if (b->cuda(aa_launch_batch_advance(b->d_counter, s), "batch counter")) return LBM_ERR_CUDA;
+  }
+  return LBM_OK;
+}
+
+void batch_free(lbm_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  cudaFree(b->d_doms);
+  cudaFree(b->d_item_dom);
+  cudaFree(b->d_counter);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t lbm_batch_create(lbm_ctx* const* ctxs, int32_t count, lbm_batch** out) {
+  if (!ctxs || !out || count < 1) return set_global(LBM_ERR_ARG, "lbm_batch_create: need at least one context");
+  *out = nullptr;
+  const lbm_ctx* c0 = ctxs[0];
+  if (!c0) return set_global(LBM_ERR_ARG, "lbm_batch_create: null context 0");
+  long long items = 0;
+  for (int32_t m = 0; m < count; m++) {
+    const lbm_ctx* c = ctxs[m];
+    if (!c) return set_global(LBM_ERR_ARG, "lbm_batch_create: null context %d", m);
+    if (c->ref) return set_global(LBM_ERR_UNSUPPORTED, "context %d: batches take config-mode domains", m);
+    if (!c->initialised) return set_global(LBM_ERR_STATE, "context %d is not initialised", m);
+    if (c->has_moving) return set_global(LBM_ERR_UNSUPPORTED, "context %d has a moving body (batches take static bodies)", m);
+    if (c->tma) return set_global(LBM_ERR_UNSUPPORTED, "context %d uses the TMA-staged step", m);
+    if (c->device != c0->device || c->stream != c0->stream)
+      return set_global(LBM_ERR_ARG, "context %d: all members share one device and one stream", m);
+    if (c->cfg.storage != c0->cfg.storage || c->cfg.collision != c0->cfg.collision)
+      return set_global(LBM_ERR_ARG, "context %d: all members share storage and collision", m);
+    for (int32_t j = 0; j < m; j++)
+      if (ctxs[j] == c) return set_global(LBM_ERR_ARG, "context %d appears twice", m);
+    items += (c->g.N + BATCH_ITEM - 1) / BATCH_ITEM;
+  }
+  if (items >= (1LL << 31)) return set_global(LBM_ERR_CAPACITY, "more than 2^31-1 work items");
+  lbm_batch* b = new lbm_batch();
+  b->ctxs.assign(ctxs, ctxs + count);
+  b->device = c0->device;
+  b->stream = c0->stream;
+  b->storage = c0->cfg.storage;
+  b->trt = c0->cfg.collision == LBM_COLL_TRT;
+  b->items = items;
+  for (lbm_ctx* c : b->ctxs) {
+    b->force = b->force || has_force(c);  // a zero acceleration adds exact zeros
+    b->faces = b->faces || has_faces(c);
+  }
+  auto bail = [&](int rc) {
+    set_global(rc, "%s", b->err.c_str());
+    batch_free(b);
+    delete b;
+    return rc;
+  };
+  if (b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) return bail(LBM_ERR_CUDA);
+  b->host.resize(count);
+  std::vector<int> item_dom((size_t)items);
+  long long next = 0;
+  for (int32_t m = 0; m < count; m++) {
+    const long long n = (ctxs[m]->g.N + BATCH_ITEM - 1) / BATCH_ITEM;
+    b->host[m].item_begin = next;
+    for (long long i = 0; i < n; i++) item_dom[(size_t)(next + i)] = m;
+    next += n;
+    batch_entry(b, m, b->host[m]);
+  }
+  int per_sm = 0, sms = 0;
+  if (b->cuda(aa_batch_blocks_per_sm(b->storage, b->trt, b->force, b->faces, &per_sm), "occupancy")) return bail(LBM_ERR_CUDA);
+  if (b->cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count")) return bail(LBM_ERR_CUDA);
+  if (per_sm < 1) return bail(b->fail(LBM_ERR_CUDA, "the batched kernel does not fit on an SM"));
+  b->blocks = (int)std::min<long long>((long long)sms * per_sm, items);
+  if (const char* env = std::getenv("LBM3D_BATCH_BLOCKS")) {
+    const int v = std::atoi(env);
+    if (v > 0) b->blocks = (int)std::min<long long>(v, items);
+  }
+  if (b->cuda(cudaMalloc(&b->d_doms, (size_t)count * sizeof(BatchDom)), "cudaMalloc(batch table)")) return bail(LBM_ERR_CUDA);
+  if (b->cuda(cudaMalloc(&b->d_item_dom, (size_t)items * sizeof(int)), "cudaMalloc(item map)")) return bail(LBM_ERR_CUDA);
+  if (b->cuda(cudaMalloc(&b->d_counter, sizeof(long long)), "cudaMalloc(counter)")) return bail(LBM_ERR_CUDA);
+  if (b->cuda(cudaMemcpy(b->d_doms, b->host.data(), (size_t)count * sizeof(BatchDom), cudaMemcpyHostToDevice), "H2D"))
+    return bail(LBM_ERR_CUDA);
+  if (b->cuda(cudaMemcpy(b->d_item_dom, item_dom.data(), (size_t)items * sizeof(int), cudaMemcpyHostToDevice), "H2D"))
+    return bail(LBM_ERR_CUDA);
+  if (b->cuda(cudaMemset(b->d_counter, 0, sizeof(long long)), "memset")) return bail(LBM_ERR_CUDA);
+  // members' earlier work (initialisation, single steps) precedes the batch
+  if (b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize")) return bail(LBM_ERR_CUDA);
+  *out = b;
+  return LBM_OK;
+}
+
+int32_t lbm_batch_destroy(lbm_batch* b) {
+  if (!b) return LBM_OK;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  batch_free(b);
+  delete b;
+  return LBM_OK;
+}
+
+const char* lbm_batch_last_error(const lbm_batch* b) { return b ? b->err.c_str() : g_error.c_str(); }
+
+int32_t lbm_batch_step(lbm_batch* b, int32_t nsteps) {
+  if (!b) return LBM_ERR_ARG;
+  if (nsteps < 0) return b->fail(LBM_ERR_ARG, "nsteps < 0");
+  if (b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  int rc = batch_refresh(b);
+  if (rc) return rc;
+  rc = batch_enqueue(b, nsteps, b->stream);
+  if (rc) return rc;
+  b->launches += 2LL * nsteps;
+  for (lbm_ctx* c : b->ctxs) c->launches += nsteps;
+  batch_advance_members(b, nsteps);
+  return LBM_OK;
+}
+
+int32_t lbm_batch_capture(lbm_batch* b, int32_t nsteps) {
+  if (!b) return LBM_ERR_ARG;
+  if (nsteps < 1) return b->fail(LBM_ERR_ARG, "nsteps < 1");
+  if (b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (!b->cap_stream &&
+      b->cuda(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
+    return LBM_ERR_CUDA;
+  if (b->cuda(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture"))
+    return LBM_ERR_CUDA;
+  const int rc = batch_enqueue(b, nsteps, b->cap_stream);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (b->cuda(e, "end capture")) return LBM_ERR_CUDA;
+  b->graph = g;
+  if (b->cuda(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate")) return LBM_ERR_CUDA;
+  b->graph_steps = nsteps;
+  return LBM_OK;
+}
+
+int32_t lbm_batch_replay(lbm_batch* b, int32_t times) {
+  if (!b) return LBM_ERR_ARG;
+  if (!b->exec) return b->fail(LBM_ERR_STATE, "no captured graph (call lbm_batch_capture first)");
+  if (times < 0) return b->fail(LBM_ERR_ARG, "times < 0");
+  if (b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  int rc = batch_refresh(b);
+  if (rc) return rc;
+  for (int32_t r = 0; r < times; r++)
+    if (b->cuda(cudaGraphLaunch(b->exec, b->stream), "cudaGraphLaunch")) return LBM_ERR_CUDA;
+  const long long n = (long long)times * b->graph_steps;
+  b->launches += 2 * n;
+  for (lbm_ctx* c : b->ctxs) c->launches += n;
+  batch_advance_members(b, n);
+  return LBM_OK;
+}
+
+int64_t lbm_batch_launch_count(const lbm_batch* b) { return b ? b->launches : -1; }
+
+int32_t lbm_batch_synchronize(lbm_batch* b) {
+  if (!b) return LBM_ERR_ARG;
+  if (b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  return b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
 }
 
 }  // extern "C"

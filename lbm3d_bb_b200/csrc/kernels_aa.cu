@@ -1,852 +1,85 @@
-// kernels_aa.cu — configurable D3Q19 step as one fused AA-pattern kernel.
-//
-// One population array A (SoA: A[d*plane + node]) is updated in place.  Steps
-// alternate between two phases:
-//   even phase: node x reads S[d,x] = A[d][x], collides, and writes its
-//               post-collision f*[dbar] into A[d][x] (swapped slots);
-//   odd phase:  node x pulls S[d,x] = A[dbar][x - c_d], collides, and pushes
-//               f*[d] into A[d][x + c_d].
-// Every slot is read and written by exactly one thread per phase, so the kernel
-// is race-free and moves 2 * 19 populations per node per step.
-//
-// Boundaries are "own-slot" rules: when the source x - c_d of an incoming
-// population lies outside a non-periodic face or in a solid node, the value is a
-// function of node x alone (bounce-back, equilibrium, zero-gradient) and is kept
-// in A[d][x], a slot no other node touches in either phase.  This covers
-// SolidBC.jl's moving-wall bounce-back (SBB!_gpu, SolidBC.jl:160-210) and the
-// face conditions of OtherBC.jl (velocity_BC!_gpu, OtherBC.jl:112-169) in the
-// configurable form.  Links are resolved from the node flag bytes (no CSR on the
-// hot path); the momentum exchange of MEA.jl:76-116 is accumulated in FP64 and
-// reduced with warp shuffles, one atomic per block and component.
-//
-// Moving bodies: the flags of the previous step decide which incoming slots hold
-// boundary values (read side), the current flags decide what is written; nodes
-// uncovered by the body are refilled with the equilibrium at the body velocity.
-// A fresh node's emitted populations toward old fluid neighbours are recomputed by
-// those neighbours (same __noinline__ routine, bit-identical), which keeps the odd
-// phase race-free.
+// kernels_aa.cu — storage dispatch of the configurable AA step (the kernels are
+// instantiated per storage in kernels_aa_fp32.cu / kernels_aa_fp64.cu /
+// kernels_aa_fp16.cu from aa_impl.cuh), the TMA tile bits and the batch counter.
 #include "lbm_internal.cuh"
 #include "lbm_kernels.h"
 
-#ifndef LBM_MINB_F32
-#define LBM_MINB_F32 4
-#endif
-
 namespace lbm {
 
-// ---- storage policies ------------------------------------------------------------
-struct StF32 {
-  using S = float;
-  using C = float;
-  static constexpr int MIN_BLOCKS = LBM_MINB_F32;  // 256 x 4 threads -> at most 64 registers
-  static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
-  static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
-};
-struct StF64 {
-  using S = double;
-  using C = double;
-  static constexpr int MIN_BLOCKS = 2;
-  static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
-  static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
-};
-// FP16 deviation from the rest equilibrium: stored h = f - w_d*rho0, computed in FP32.
-struct StF16 {
-  using S = __half;
-  using C = float;
-  static constexpr int MIN_BLOCKS = LBM_MINB_F32;
-  static __device__ __forceinline__ C ld(const S* p, int d, C rho0) {
-    return wgt<float>(d) * rho0 + __half2float(*p);
-  }
-  static __device__ __forceinline__ void st(S* p, C v, int d, C rho0) {
-    *p = __float2half_rn(v - wgt<float>(d) * rho0);
-  }
-};
+#define LBM_AA_DECLARE_OPS(NAME)                                                                                  \
+  cudaError_t aa_step_##NAME(const AAParams& p, void* A, const uint8_t* flags, bool odd, bool trt, bool force,    \
+                             bool faces, dim3 grid, dim3 block, cudaStream_t s);                                  \
+  cudaError_t aa_batch_##NAME(const BatchParams& bp, bool trt, bool force, bool faces, int blocks, int* per_sm,  \
+                              cudaStream_t s);                                                                    \
+  cudaError_t aa_export_##NAME(const ReadParams& p, const void* A, const uint8_t* flags, const ExportOut& out,    \
+                               dim3 grid, dim3 block, cudaStream_t s);                                            \
+  cudaError_t aa_reduce_##NAME(const ReadParams& p, const void* A, const uint8_t* flags, double* out, dim3 grid,  \
+                               dim3 block, cudaStream_t s);                                                       \
+  cudaError_t aa_init_##NAME(const InitParams& p, void* A, const uint8_t* flags, dim3 grid, dim3 block,           \
+                             cudaStream_t s);
+LBM_AA_DECLARE_OPS(fp32)
+LBM_AA_DECLARE_OPS(fp64)
+LBM_AA_DECLARE_OPS(fp16)
+#undef LBM_AA_DECLARE_OPS
 
-// ---- collision ---------------------------------------------------------------------
-template <class C>
-struct Coll {
-  C om_p, om_m;  // relaxation rates
-  C gx, gy, gz;  // body acceleration
-};
-
-// 1/rho: one MUFU instruction in FP32 (rho is O(1), the ~1 ulp error is far below
-// the storage precision); exact division in FP64.
-__device__ __forceinline__ float recip(float r) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(r));
-  return y;
-}
-__device__ __forceinline__ double recip(double r) { return 1.0 / r; }
-
-// Moments from the nine opposite-direction pairs (d, d+1): s = f_d + f_{d+1},
-// t = f_d - f_{d+1}; rho = sum s + f_18, j = sum over pairs of c_d t.  Then
-// u = j/rho + g/2 (Guo).
-template <class C, bool FORCE>
-__device__ __forceinline__ void moments(const C* f, const Coll<C>& k, C& rho, C& ux, C& uy, C& uz) {
-  C sp[9], tp[9];
-#pragma unroll
-  for (int q = 0; q < 9; q++) {
-    sp[q] = f[2 * q] + f[2 * q + 1];
-    tp[q] = f[2 * q] - f[2 * q + 1];
+cudaError_t aa_launch_step(int storage, const AAParams& p, void* A, const uint8_t* flags, bool odd, bool trt,
+                           bool force, bool faces, dim3 grid, dim3 block, cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32: return aa_step_fp32(p, A, flags, odd, trt, force, faces, grid, block, s);
+    case LBM_STORE_FP64: return aa_step_fp64(p, A, flags, odd, trt, force, faces, grid, block, s);
+    case LBM_STORE_FP16DEV: return aa_step_fp16(p, A, flags, odd, trt, force, faces, grid, block, s);
   }
-  C r = ((sp[0] + sp[1]) + (sp[2] + sp[3])) + ((sp[4] + sp[5]) + (sp[6] + sp[7])) + (sp[8] + f[18]);
-  C jx = C(0), jy = C(0), jz = C(0);
-#pragma unroll
-  for (int q = 0; q < 9; q++) {
-    const int d = 2 * q;
-    if (cx(d) == 1) jx += tp[q];
-    if (cx(d) == -1) jx -= tp[q];
-    if (cy(d) == 1) jy += tp[q];
-    if (cy(d) == -1) jy -= tp[q];
-    if (cz(d) == 1) jz += tp[q];
-    if (cz(d) == -1) jz -= tp[q];
-  }
-  const C inv = recip(r);
-  rho = r;
-  ux = jx * inv;
-  uy = jy * inv;
-  uz = jz * inv;
-  if (FORCE) {
-    ux += C(0.5) * k.gx;
-    uy += C(0.5) * k.gy;
-    uz += C(0.5) * k.gz;
-  }
+  return cudaErrorInvalidValue;
 }
 
-template <class C>
-__device__ __forceinline__ C cdot(int d, C ux, C uy, C uz) {
-  C s = C(0);
-  if (cx(d) == 1) s += ux;
-  if (cx(d) == -1) s -= ux;
-  if (cy(d) == 1) s += uy;
-  if (cy(d) == -1) s -= uy;
-  if (cz(d) == 1) s += uz;
-  if (cz(d) == -1) s -= uz;
-  return s;
+cudaError_t aa_launch_batch(int storage, const BatchParams& bp, bool trt, bool force, bool faces, int blocks,
+                            cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32: return aa_batch_fp32(bp, trt, force, faces, blocks, nullptr, s);
+    case LBM_STORE_FP64: return aa_batch_fp64(bp, trt, force, faces, blocks, nullptr, s);
+    case LBM_STORE_FP16DEV: return aa_batch_fp16(bp, trt, force, faces, blocks, nullptr, s);
+  }
+  return cudaErrorInvalidValue;
 }
 
-template <class C>
-__device__ __forceinline__ C feq(int d, C rho, C ux, C uy, C uz) {
-  C cu = cdot<C>(d, ux, uy, uz);
-  C usq = ux * ux + uy * uy + uz * uz;
-  return wgt<C>(d) * rho * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * usq);
+cudaError_t aa_batch_blocks_per_sm(int storage, bool trt, bool force, bool faces, int* per_sm) {
+  BatchParams none{};
+  switch (storage) {
+    case LBM_STORE_FP32: return aa_batch_fp32(none, trt, force, faces, 0, per_sm, nullptr);
+    case LBM_STORE_FP64: return aa_batch_fp64(none, trt, force, faces, 0, per_sm, nullptr);
+    case LBM_STORE_FP16DEV: return aa_batch_fp16(none, trt, force, faces, 0, per_sm, nullptr);
+  }
+  return cudaErrorInvalidValue;
 }
 
-// BGK / TRT with Guo forcing, f -> p, written per opposite pair (d, d+1) with
-// c_{d+1} = -c_d: the equilibrium splits into an even part
-// e = w rho (1 - 1.5 u^2 + 4.5 (c.u)^2) and an odd part o = 3 w rho (c.u), the Guo
-// source S_d = w [3 (c_d - u).F + 9 (c_d.u)(c_d.F)] into w (9 (c.u)(c.F) - 3 u.F) and
-// 3 w (c.F).  Relaxation rates and weights are folded per weight class.
-template <class C, bool TRT, bool FORCE>
-__device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rho, C ux, C uy, C uz) {
-  const C usq = ux * ux + uy * uy + uz * uz;
-  const C base = C(1) - C(1.5) * usq;
-  C Fx = C(0), Fy = C(0), Fz = C(0), m3uF = C(0);
-  if (FORCE) {
-    Fx = rho * k.gx;
-    Fy = rho * k.gy;
-    Fz = rho * k.gz;
-    m3uF = C(-3) * (ux * Fx + uy * Fy + uz * Fz);
+cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
+                             const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32: return aa_export_fp32(p, A, flags, out, grid, block, s);
+    case LBM_STORE_FP64: return aa_export_fp64(p, A, flags, out, grid, block, s);
+    case LBM_STORE_FP16DEV: return aa_export_fp16(p, A, flags, out, grid, block, s);
   }
-  const C wr1 = rho * wgt<C>(0), wr2 = rho * wgt<C>(6), wr0 = rho * wgt<C>(18);
-  if (!TRT) {
-    const C om = k.om_p, omc = C(1) - k.om_p;
-    // omega * e = B + T (c.u)^2 ; omega * o = O (c.u)
-    const C B1 = om * wr1 * base, B2 = om * wr2 * base;
-    const C T1 = C(4.5) * om * wr1, T2 = C(4.5) * om * wr2;
-    const C O1 = C(3) * om * wr1, O2 = C(3) * om * wr2;
-    const C fac = C(1) - C(0.5) * om;
-    const C G1 = fac * wgt<C>(0), G2 = fac * wgt<C>(6);
-#pragma unroll
-    for (int q = 0; q < 9; q++) {
-      const int d = 2 * q;
-      const bool c1 = d < 6;
-      const C cu = cdot<C>(d, ux, uy, uz);
-      C e = (c1 ? T1 : T2) * (cu * cu) + (c1 ? B1 : B2);
-      C o = (c1 ? O1 : O2) * cu;
-      if (FORCE) {
-        const C cF = cdot<C>(d, Fx, Fy, Fz);
-        const C G = c1 ? G1 : G2;
-        e += G * (C(9) * (cu * cF) + m3uF);
-        o += (C(3) * G) * cF;
-      }
-      p[d] = omc * f[d] + (e + o);
-      p[d + 1] = omc * f[d + 1] + (e - o);
-    }
-    C e0 = om * wr0 * base;
-    if (FORCE) e0 += fac * wgt<C>(18) * m3uF;
-    p[18] = omc * f[18] + e0;
-  } else {
-    const C hp = C(0.5) * k.om_p, hm = C(0.5) * k.om_m;
-    const C fac_p = C(1) - hp, fac_m = C(1) - hm;
-#pragma unroll
-    for (int q = 0; q < 9; q++) {
-      const int d = 2 * q;
-      const C wr = d < 6 ? wr1 : wr2;
-      const C cu = cdot<C>(d, ux, uy, uz);
-      C e = wr * (base + C(4.5) * (cu * cu));
-      C o = (C(3) * wr) * cu;
-      // A = om_p (f+ - e), Bm = om_m (f- - o), f+- = (f_d +- f_d+1)/2
-      C A = hp * (f[d] + f[d + 1]) - k.om_p * e;
-      C Bm = hm * (f[d] - f[d + 1]) - k.om_m * o;
-      if (FORCE) {
-        const C w = wgt<C>(d);
-        const C cF = cdot<C>(d, Fx, Fy, Fz);
-        A -= fac_p * w * (C(9) * (cu * cF) + m3uF);
-        Bm -= fac_m * (C(3) * w) * cF;
-      }
-      p[d] = (f[d] - A) - Bm;
-      p[d + 1] = (f[d + 1] - A) + Bm;
-    }
-    C v = f[18] - k.om_p * (f[18] - wr0 * base);
-    if (FORCE) v += fac_p * wgt<C>(18) * m3uF;
-    p[18] = v;
-  }
+  return cudaErrorInvalidValue;
 }
 
-// Wall velocity of the moving body at lattice point (px,py,pz).
-__device__ __forceinline__ void wall_velocity(const Kinematics& k, double px, double py, double pz,
-                                              double& wx, double& wy, double& wz) {
-  const double rx = px - k.center[0], ry = py - k.center[1], rz = pz - k.center[2];
-  wx = k.vel[0] + (k.omega[1] * rz - k.omega[2] * ry);
-  wy = k.vel[1] + (k.omega[2] * rx - k.omega[0] * rz);
-  wz = k.vel[2] + (k.omega[0] * ry - k.omega[1] * rx);
+cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags, double* out,
+                             dim3 grid, dim3 block, cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32: return aa_reduce_fp32(p, A, flags, out, grid, block, s);
+    case LBM_STORE_FP64: return aa_reduce_fp64(p, A, flags, out, grid, block, s);
+    case LBM_STORE_FP16DEV: return aa_reduce_fp16(p, A, flags, out, grid, block, s);
+  }
+  return cudaErrorInvalidValue;
 }
 
-// Post-collision state of a node refilled with feq(rho0, u_wall(node)).  Not
-// inlined: a fresh node and each of its old-fluid neighbours call the same code
-// and therefore obtain bit-identical values.
-template <class C, bool TRT, bool FORCE>
-__device__ __noinline__ void fresh_state(Coll<C> k, Kinematics kin, C rho0, int x, int y, int z,
-                                         C* p, C* mom) {
-  double wx, wy, wz;
-  wall_velocity(kin, x + 0.5, y + 0.5, z + 0.5, wx, wy, wz);
-  C f[Q];
-#pragma unroll
-  for (int d = 0; d < Q; d++) f[d] = feq<C>(d, rho0, C(wx), C(wy), C(wz));
-  C rho, ux, uy, uz;
-  moments<C, FORCE>(f, k, rho, ux, uy, uz);
-  collide<C, TRT, FORCE>(f, p, k, rho, ux, uy, uz);
-  mom[0] = rho;
-  mom[1] = ux;
-  mom[2] = uy;
-  mom[3] = uz;
-}
-
-// ---- the step kernel ------------------------------------------------------------------
-// General path of one fluid node: faces, solid links, moving-body refill, momentum
-// exchange.  Kept out of line so that its register demand does not limit the
-// occupancy of the interior fast path; only warps containing a boundary node run it.
-template <class SP, bool ODD, bool TRT, bool FORCE>
-__device__ __noinline__ void aa_general(const AAParams& p, typename SP::S* __restrict__ A,
-                                        const uint8_t* __restrict__ flags, const int x, const int y,
-                                        const int z, const long long i, const uint8_t fl, double* acc,
-                                        bool* has_out) {
-  using C = typename SP::C;
-  const Grid& g = p.g;
-  const C rho0 = C(p.rho0);
-  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
-  bool has_link = false;
-  const long long nxl = g.nx, nxy = (long long)g.nx * g.ny;
-  // neighbour coordinates; -1 when outside a non-periodic axis
-  const int xs0 = x == 0 ? (g.per[0] ? g.nx - 1 : -1) : x - 1;
-  const int xs2 = x == g.nx - 1 ? (g.per[0] ? 0 : -1) : x + 1;
-  const int ys0 = y == 0 ? (g.per[1] ? g.ny - 1 : -1) : y - 1;
-  const int ys2 = y == g.ny - 1 ? (g.per[1] ? 0 : -1) : y + 1;
-  const int zs0 = z == 0 ? (g.per[2] ? g.nz - 1 : -1) : z - 1;
-  const int zs2 = z == g.nz - 1 ? (g.per[2] ? 0 : -1) : z + 1;
-  const int xs[3] = {xs0, x, xs2}, ys[3] = {ys0, y, ys2}, zs[3] = {zs0, z, zs2};
-  const bool on_face = (xs0 | xs2 | ys0 | ys2 | zs0 | zs2) < 0;
-  const bool near = (fl & F_NEAR) != 0;
-
-  uint32_t face = 0, bcp = 0, bcc = 0, mov = 0;
-  if (on_face || near) {
-#pragma unroll
-    for (int d = 0; d < 18; d++) {
-      const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
-      if ((sx | sy | sz) < 0) {
-        face |= 1u << d;
-      } else if (near) {
-        const uint8_t fs = flags[sx + nxl * sy + nxy * sz];
-        if (fs & F_SOLID_PREV) bcp |= 1u << d;
-        if (fs & F_SOLID) bcc |= 1u << d;
-        if (fs & F_MOVING) mov |= 1u << d;
-      }
-    }
+cudaError_t aa_launch_init(int storage, const InitParams& p, void* A, const uint8_t* flags, dim3 grid, dim3 block,
+                           cudaStream_t s) {
+  switch (storage) {
+    case LBM_STORE_FP32: return aa_init_fp32(p, A, flags, grid, block, s);
+    case LBM_STORE_FP64: return aa_init_fp64(p, A, flags, grid, block, s);
+    case LBM_STORE_FP16DEV: return aa_init_fp16(p, A, flags, grid, block, s);
   }
-  const uint32_t bcr = face | bcp;  // incoming slots holding boundary values (read side)
-  const uint32_t bcw = face | bcc;  // incoming slots to fill with boundary values (write side)
-  const bool fresh = (fl & F_SOLID_PREV) != 0;
-
-  C pst[Q];
-  C rho, ux, uy, uz;
-  if (!fresh) {
-    C f[Q];
-#pragma unroll
-    for (int d = 0; d < Q; d++) {
-      long long a;
-      if (!ODD || d == 18) {
-        a = (long long)d * g.plane + i;
-      } else {
-        const long long src = xs[1 - cx(d)] + nxl * ys[1 - cy(d)] + nxy * zs[1 - cz(d)];
-        a = ((bcr >> d) & 1u) ? (long long)d * g.plane + i : (long long)opp(d) * g.plane + src;
-      }
-      f[d] = SP::ld(A + a, d, rho0);
-    }
-    moments<C, FORCE>(f, k, rho, ux, uy, uz);
-    collide<C, TRT, FORCE>(f, pst, k, rho, ux, uy, uz);
-  } else {
-    C mom[4];
-    fresh_state<C, TRT, FORCE>(k, p.kin, rho0, x, y, z, pst, mom);
-    rho = mom[0];
-    ux = mom[1];
-    uy = mom[2];
-    uz = mom[3];
-  }
-
-  // boundary value of incoming direction d (own slot A[d][x])
-  auto bcval = [&](const int d) -> C {
-    const int o = opp(d);
-    if ((face >> d) & 1u) {
-      // face of the missing source: x first, then y, then z (static indices only)
-      const bool xo = (cx(d) > 0 && xs0 < 0) || (cx(d) < 0 && xs2 < 0);
-      const bool yo = (cy(d) > 0 && ys0 < 0) || (cy(d) < 0 && ys2 < 0);
-      const int fx = cx(d) > 0 ? 0 : 1, fy = cy(d) > 0 ? 2 : 3, fz = cz(d) > 0 ? 4 : 5;
-      const int kind = xo ? p.face_kind[fx] : (yo ? p.face_kind[fy] : p.face_kind[fz]);
-      const C ufx = C(xo ? p.face_u[fx][0] : (yo ? p.face_u[fy][0] : p.face_u[fz][0]));
-      const C ufy = C(xo ? p.face_u[fx][1] : (yo ? p.face_u[fy][1] : p.face_u[fz][1]));
-      const C ufz = C(xo ? p.face_u[fx][2] : (yo ? p.face_u[fy][2] : p.face_u[fz][2]));
-      if (kind == LBM_FACE_EQ_INLET) return feq<C>(d, rho, ufx, ufy, ufz);
-      if (kind == LBM_FACE_OUTFLOW) return pst[d];
-      return pst[o] - C(6) * wgt<C>(o) * rho * cdot<C>(o, ufx, ufy, ufz);
-    }
-    C cdu = C(0);
-    if ((mov >> d) & 1u) {
-      double wx, wy, wz;
-      wall_velocity(p.kin, x + 0.5 + 0.5 * cx(o), y + 0.5 + 0.5 * cy(o), z + 0.5 + 0.5 * cz(o), wx,
-                    wy, wz);
-      cdu = cdot<C>(o, C(wx), C(wy), C(wz));
-    }
-    const C v = pst[o] - C(6) * wgt<C>(o) * rho * cdu;
-    if (p.compute_force) {
-      // momentum exchange of link (x, o): c_o (f*_o + f_in)
-      const double t = (double)pst[o] + (double)v;
-      const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
-      const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
-      const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
-      const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
-      acc[0] += fx;
-      acc[1] += fy;
-      acc[2] += fz;
-      acc[3] += ry * fz - rz * fy;
-      acc[4] += rz * fx - rx * fz;
-      acc[5] += rx * fy - ry * fx;
-      has_link = true;
-    }
-    return v;
-  };
-
-  if (!ODD) {
-#pragma unroll
-    for (int d = 0; d < Q; d++) {
-      C v;
-      if ((bcw >> d) & 1u) v = bcval(d);
-      else v = pst[opp(d)];
-      SP::st(A + (long long)d * g.plane + i, v, d, rho0);
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < Q; j++) {
-      const int o = opp(j);
-      if ((bcw >> o) & 1u) {
-        // target x + c_j is outside/solid: the boundary value of incoming o goes to A[o][x]
-        const C v = bcval(o);
-        SP::st(A + (long long)o * g.plane + i, v, o, rho0);
-      } else if (j == 18 || !fresh || ((bcp >> o) & 1u)) {
-        // a fresh node leaves its emission toward old-fluid targets to them
-        const long long tgt = xs[1 + cx(j)] + nxl * ys[1 + cy(j)] + nxy * zs[1 + cz(j)];
-        SP::st(A + (long long)j * g.plane + tgt, pst[j], j, rho0);
-      }
-    }
-    if (!fresh) {
-      const uint32_t fnb = bcp & ~bcc & ~face;  // neighbours uncovered this step
-      if (fnb) {
-#pragma unroll
-        for (int d = 0; d < 18; d++) {
-          if (!((fnb >> d) & 1u)) continue;
-          // source coordinates of direction d (x - c_d), wrapped
-          const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
-          C q[Q], mom[4];
-          fresh_state<C, TRT, FORCE>(k, p.kin, rho0, sx, sy, sz, q, mom);
-          C qd = q[0];
-#pragma unroll
-          for (int e = 1; e < Q; e++)
-            if (e == d) qd = q[e];
-          SP::st(A + (long long)d * g.plane + i, qd, d, rho0);
-        }
-      }
-    }
-  }
-  *has_out = *has_out || has_link;
-}
-
-// Fast path: interior node whose only boundaries are static no-slip links (bc =
-// incoming directions whose source is solid; 0 for most nodes).  Neighbour offsets
-// are precomputed on the host (p.off_rd / p.off_wr); the periodic x wrap is patched
-// per lane.  A static no-slip bounce-back value for incoming d is f*_{opp(d)}: in
-// the even phase that is exactly the swapped store, in the odd phase it only
-// redirects the store of f*_j from the solid target x + c_j to the own slot opp(j).
-//
-// The loads are split from the compute so that the caller can issue them before the
-// node's flag byte arrives (speculatively, for every lane whose coordinates allow
-// the fast path), instead of chaining two memory round trips.
-template <class SP, bool ODD>
-__device__ __forceinline__ void aa_fast_load(const AAParams& p, const typename SP::S* __restrict__ base,
-                                             const int x, typename SP::C* f) {
-  using C = typename SP::C;
-  const C rho0 = C(p.rho0);
-  long long fix_lo = 0, fix_hi = 0;  // periodic x wrap at the row ends (odd phase)
-  if (ODD) {
-    fix_lo = x == 0 ? (long long)p.g.nx : 0;
-    fix_hi = x == p.g.nx - 1 ? (long long)p.g.nx : 0;
-  }
-#pragma unroll
-  for (int d = 0; d < Q; d++) {
-    long long o = p.off_rd[d];
-    if (ODD) {
-      if (cx(d) == 1) o += fix_lo;
-      if (cx(d) == -1) o -= fix_hi;
-    }
-    f[d] = SP::ld(base + o, d, rho0);
-  }
-}
-
-template <class SP, bool ODD, bool TRT, bool FORCE>
-__device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S* __restrict__ base,
-                                               const int x, const int y, const int z, const uint32_t bc,
-                                               typename SP::C* f, double* acc, bool* has_link) {
-  using C = typename SP::C;
-  const C rho0 = C(p.rho0);
-  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
-  if (ODD && bc) {  // bounce-back values are kept in the own slots
-#pragma unroll
-    for (int d = 0; d < 18; d++)
-      if ((bc >> d) & 1u) f[d] = SP::ld(base + (long long)d * p.g.plane, d, rho0);
-  }
-  long long fix_lo = 0, fix_hi = 0;
-  if (ODD) {
-    fix_lo = x == 0 ? (long long)p.g.nx : 0;
-    fix_hi = x == p.g.nx - 1 ? (long long)p.g.nx : 0;
-  }
-  C rho, ux, uy, uz;
-  moments<C, FORCE>(f, k, rho, ux, uy, uz);
-  C pst[Q];
-  collide<C, TRT, FORCE>(f, pst, k, rho, ux, uy, uz);
-#pragma unroll
-  for (int j = 0; j < Q; j++) {
-    long long o = p.off_wr[j];
-    if (ODD) {
-      if (cx(j) == 1) o -= fix_hi;
-      if (cx(j) == -1) o += fix_lo;
-      if (j < 18 && ((bc >> opp(j)) & 1u)) o = (long long)opp(j) * p.g.plane;
-    }
-    SP::st(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
-  }
-  if (bc && p.compute_force) {
-    // momentum exchange of the static links: c_o (f*_o + f*_o), o = opp(d)
-#pragma unroll
-    for (int d = 0; d < 18; d++) {
-      if (!((bc >> d) & 1u)) continue;
-      const int o = opp(d);
-      const double t = 2.0 * (double)pst[o];
-      const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
-      const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
-      const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
-      const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
-      acc[0] += fx;
-      acc[1] += fy;
-      acc[2] += fz;
-      acc[3] += ry * fz - rz * fy;
-      acc[4] += rz * fx - rx * fz;
-      acc[5] += rx * fy - ry * fx;
-    }
-    *has_link = true;
-  }
-}
-
-// One node on the direct path: lanes whose coordinates allow the fast path issue
-// their population loads at once; the flag byte (and, next to a solid, the link
-// word) decides afterwards whether the warp finishes on the fast path or reruns the
-// node on the general path.  All 32 lanes of a warp reach the vote.
-template <class SP, bool ODD, bool TRT, bool FORCE>
-__device__ __forceinline__ void aa_direct(const AAParams& p, typename SP::S* __restrict__ A,
-                                          const uint8_t* __restrict__ flags, const int x, const int y, const int z,
-                                          const bool inb, double* acc, bool* has_link) {
-  using C = typename SP::C;
-  const Grid& g = p.g;
-  const long long i = inb ? node_index(g, x, y, z) : 0;
-  const bool xin = g.per[0] || (x > 0 && x < g.nx - 1);
-  bool coord_fast = inb && xin;
-  if (ODD) {
-    coord_fast = coord_fast && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
-  } else {
-    coord_fast = coord_fast && (g.per[1] || (y > 0 && y < g.ny - 1)) && (g.per[2] || (z > 0 && z < g.nz - 1));
-  }
-  const uint8_t fl = inb ? flags[i] : (uint8_t)F_SOLID;
-  C f[Q];
-  if (coord_fast) aa_fast_load<SP, ODD>(p, A + i, x, f);  // in-bounds: interior in every non-wrapped axis
-  const bool solid = (fl & F_SOLID) != 0;
-  // fast when the only boundaries are static no-slip links (link word: current ==
-  // previous links, no moving-body link, not uncovered)
-  uint32_t bc = 0;
-  bool static_links = true;
-  if (!solid && (fl & F_NEAR)) {
-    const unsigned long long lw = p.links[i];
-    const uint32_t cur = (uint32_t)(lw & 0x3FFFFu), prev = (uint32_t)((lw >> 18) & 0x3FFFFu);
-    const uint32_t mov = (uint32_t)((lw >> 36) & 0x3FFFFu);
-    static_links = cur == prev && mov == 0 && !(fl & F_SOLID_PREV);
-    bc = cur;
-  }
-  const bool fast = coord_fast && static_links;
-  const bool warp_fast = __all_sync(0xffffffffu, solid || fast);
-  if (warp_fast) {
-    if (!solid) aa_fast_finish<SP, ODD, TRT, FORCE>(p, A + i, x, y, z, bc, f, acc, has_link);
-  } else if (!solid) {
-    aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, i, fl, acc, has_link);
-  }
-}
-
-template <class SP, bool ODD, bool TRT, bool FORCE>
-__global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __grid_constant__ AAParams p,
-                                                                      typename SP::S* __restrict__ A,
-                                                                      const uint8_t* __restrict__ flags) {
-  const Grid& g = p.g;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const bool inb = (x < g.nx) && (y < g.ny);
-  clear_record(p.zero_next);  // the next step's force record (read by the next launch only)
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  bool has_link = false;
-  aa_direct<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, inb, acc, &has_link);
-  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
-}
-
-// ---- TMA-staged persistent step ------------------------------------------------------
-// Tiles are row segments of TW cells.  For every tile without a boundary node, one
-// thread streams the 19 direction segments it needs (even phase: the node's own
-// slots; odd phase: the neighbour slots, row-shifted, plus a 16-byte halo for the
-// x-shifted directions) into shared memory with cp.async.bulk, several tiles ahead,
-// completion tracked by one mbarrier per stage.  The compute reads shared memory,
-// so loads stay in flight while warps compute.  Tiles holding a boundary node are
-// processed by the direct path.
-__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
-  return (uint32_t)__cvta_generic_to_shared(ptr);
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-// Bounded wait on an mbarrier phase: gives up after ~2^22 polls (each try_wait
-// blocks for a hardware-defined interval), returning false.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); it++) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-constexpr int TMA_MAX_STAGES = 8;
-
-template <class SP, bool ODD>
-__device__ __forceinline__ void tma_issue(const AAParams& p, const typename SP::S* A, long long tile,
-                                          unsigned char* stage, uint32_t bar) {
-  using S = typename SP::S;
-  const Grid& g = p.g;
-  const TmaCfg& T = p.tma;
-  const int tw = T.tw, H = T.halo;
-  const long long row = tile / T.ntx;
-  const int x0 = (int)(tile - row * T.ntx) * tw;
-  const int y = (int)(row % g.ny), z = (int)(row / g.ny);
-  const uint32_t seg = (uint32_t)(tw * sizeof(S)), hal = 16u;
-  mbar_expect_tx(bar, ODD ? 19u * seg + 10u * hal : 19u * seg);
-  const uint32_t dst0 = smem_u32(stage);
-  const uint32_t dstride = (uint32_t)(T.buf_elems * sizeof(S));
-#pragma unroll 1
-  for (int d = 0; d < Q; d++) {
-    const uint32_t dst = dst0 + d * dstride;
-    if (!ODD) {
-      bulk_g2s(dst, A + (long long)d * g.plane + row * g.nx + x0, seg, bar);
-      continue;
-    }
-    int ys = y - cy(d), zs = z - cz(d);
-    ys = ys < 0 ? ys + g.ny : (ys >= g.ny ? ys - g.ny : ys);
-    zs = zs < 0 ? zs + g.nz : (zs >= g.nz ? zs - g.nz : zs);
-    const S* rowp = A + (long long)opp(d) * g.plane + ((long long)zs * g.ny + ys) * g.nx;
-    const int c = cx(d);
-    if (c == 0) {
-      bulk_g2s(dst, rowp + x0, seg, bar);
-    } else if (c == 1) {  // source x-1: [halo | main]
-      bulk_g2s(dst, rowp + (x0 >= H ? x0 - H : g.nx - H), hal, bar);
-      bulk_g2s(dst + hal, rowp + x0, seg, bar);
-    } else {  // source x+1: [main | halo]
-      bulk_g2s(dst, rowp + x0, seg, bar);
-      bulk_g2s(dst + seg, rowp + (x0 + tw < g.nx ? x0 + tw : 0), hal, bar);
-    }
-  }
-}
-
-template <class SP, bool ODD, bool TRT, bool FORCE>
-__global__ void __launch_bounds__(128) aa_tma_kernel(const __grid_constant__ AAParams p,
-                                                     typename SP::S* __restrict__ A,
-                                                     const uint8_t* __restrict__ flags) {
-  using S = typename SP::S;
-  using C = typename SP::C;
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) unsigned long long bars[TMA_MAX_STAGES];
-  const Grid& g = p.g;
-  const TmaCfg& T = p.tma;
-  const int t = threadIdx.x;
-  const int NS = T.stages;
-  const long long G = gridDim.x;
-  const long long first = blockIdx.x;
-  const long long ntb = first < T.ntiles ? (T.ntiles - first + G - 1) / G : 0;
-  const uint8_t slow_bit = ODD ? 2 : 1;
-  clear_record(p.zero_next);
-  if (t == 0) {
-    for (int s = 0; s < NS; s++) mbar_init(smem_u32(&bars[s]), 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  uint32_t pending = 0;  // thread 0: stages with loads in flight
-  auto issue = [&](long long k) {
-    if (k >= ntb) return;
-    const long long tile = first + k * G;
-    if (T.tile_slow[tile] & slow_bit) return;
-    const int s = (int)(k % NS);
-    tma_issue<SP, ODD>(p, A, tile, smem + (size_t)s * T.stage_bytes, smem_u32(&bars[s]));
-    pending |= 1u << s;
-  };
-  if (t == 0)
-    for (long long k = 0; k < NS - 1; k++) issue(k);
-  uint32_t phases = 0;
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  bool has_link = false;
-  bool failed = false;
-  const C rho0 = C(p.rho0);
-  const Coll<C> kc{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
-  for (long long k = 0; k < ntb; k++) {
-    const long long tile = first + k * G;
-    const int s = (int)(k % NS);
-    if (t == 0) issue(k + NS - 1);
-    const long long row = tile / T.ntx;
-    const int x0 = (int)(tile - row * T.ntx) * T.tw;
-    const int y = (int)(row % g.ny), z = (int)(row / g.ny);
-    const int x = x0 + t;
-    if (T.tile_slow[tile] & slow_bit) {
-      aa_direct<SP, ODD, TRT, FORCE>(p, A, flags, x, y, z, true, acc, &has_link);
-      continue;
-    }
-    const bool ok = mbar_wait(smem_u32(&bars[s]), (phases >> s) & 1u);
-    phases ^= 1u << s;
-    const S* st = (const S*)(smem + (size_t)s * T.stage_bytes);
-    C f[Q];
-#pragma unroll
-    for (int d = 0; d < Q; d++) {
-      int idx = t;
-      if (ODD) idx = cx(d) == 1 ? T.halo - 1 + t : (cx(d) == -1 ? t + 1 : t);
-      f[d] = SP::ld(st + d * T.buf_elems + idx, d, rho0);
-    }
-    if (t == 0) pending &= ~(1u << s);
-    if (!__syncthreads_and(ok)) {  // stage consumed (or a wait gave up everywhere)
-      failed = true;
-      break;
-    }
-    C rho, ux, uy, uz;
-    moments<C, FORCE>(f, kc, rho, ux, uy, uz);
-    C pst[Q];
-    collide<C, TRT, FORCE>(f, pst, kc, rho, ux, uy, uz);
-    const long long i = row * g.nx + x;
-    S* const base = A + i;
-    long long fix_lo = 0, fix_hi = 0;
-    if (ODD) {
-      fix_lo = x == 0 ? (long long)g.nx : 0;
-      fix_hi = x == g.nx - 1 ? (long long)g.nx : 0;
-    }
-#pragma unroll
-    for (int j = 0; j < Q; j++) {
-      long long o = p.off_wr[j];
-      if (ODD) {
-        if (cx(j) == 1) o -= fix_hi;
-        if (cx(j) == -1) o += fix_lo;
-      }
-      SP::st(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
-    }
-  }
-  if (failed) {
-    if (t == 0) {
-      atomicExch(T.err, 1);
-      // drain the copies this block still has in flight (bounded)
-      for (int s = 0; s < NS; s++)
-        if (pending & (1u << s)) mbar_wait(smem_u32(&bars[s]), (phases >> s) & 1u);
-    }
-    __syncthreads();
-  }
-  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
-}
-
-// ---- state readout (populations, macros, mass, finiteness) ---------------------------
-// Reconstructs S_n[d, x] from the current layout using the flag bit `solid_bit`
-// (the flags of the last completed step).
-template <class SP>
-__device__ __forceinline__ void aa_read(const ReadParams& p, const typename SP::S* A, const uint8_t* flags,
-                                        int x, int y, int z, long long i, typename SP::C* f) {
-  using C = typename SP::C;
-  const Grid& g = p.g;
-  const C rho0 = C(p.rho0);
-  if (!p.swapped) {
-#pragma unroll
-    for (int d = 0; d < Q; d++) f[d] = SP::ld(A + (long long)d * g.plane + i, d, rho0);
-    return;
-  }
-  const long long nxl = g.nx, nxy = (long long)g.nx * g.ny;
-  const int xs[3] = {x == 0 ? (g.per[0] ? g.nx - 1 : -1) : x - 1, x,
-                     x == g.nx - 1 ? (g.per[0] ? 0 : -1) : x + 1};
-  const int ys[3] = {y == 0 ? (g.per[1] ? g.ny - 1 : -1) : y - 1, y,
-                     y == g.ny - 1 ? (g.per[1] ? 0 : -1) : y + 1};
-  const int zs[3] = {z == 0 ? (g.per[2] ? g.nz - 1 : -1) : z - 1, z,
-                     z == g.nz - 1 ? (g.per[2] ? 0 : -1) : z + 1};
-#pragma unroll
-  for (int d = 0; d < Q; d++) {
-    long long a = (long long)d * g.plane + i;
-    if (d != 18) {
-      const int sx = xs[1 - cx(d)], sy = ys[1 - cy(d)], sz = zs[1 - cz(d)];
-      if ((sx | sy | sz) >= 0) {
-        const long long src = sx + nxl * sy + nxy * sz;
-        if (!(flags[src] & p.solid_bit)) a = (long long)opp(d) * g.plane + src;
-      }
-    }
-    f[d] = SP::ld(A + a, d, rho0);
-  }
-}
-
-template <class SP>
-__global__ void aa_export_kernel(const ReadParams p, const typename SP::S* __restrict__ A,
-                                 const uint8_t* __restrict__ flags, ExportOut out) {
-  using C = typename SP::C;
-  const Grid& g = p.g;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny) return;
-  const long long i = node_index(g, x, y, z);
-  C f[Q];
-  const bool solid = (flags[i] & p.solid_bit) != 0;
-  if (solid) {
-#pragma unroll
-    for (int d = 0; d < Q; d++) f[d] = C(0);
-  } else {
-    aa_read<SP>(p, A, flags, x, y, z, i, f);
-  }
-  export_node<C>(out, g, i, f, solid, p.gacc);
-}
-
-template <class SP>
-__global__ void aa_reduce_kernel(const ReadParams p, const typename SP::S* __restrict__ A,
-                                 const uint8_t* __restrict__ flags, double* out) {
-  using C = typename SP::C;
-  const Grid& g = p.g;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  bool has = false;
-  if (x < g.nx && y < g.ny) {
-    const long long i = node_index(g, x, y, z);
-    if (!(flags[i] & p.solid_bit)) {
-      C f[Q];
-      aa_read<SP>(p, A, flags, x, y, z, i, f);
-      double m = 0.0;
-      bool bad = false;
-#pragma unroll
-      for (int d = 0; d < Q; d++) {
-        m += (double)f[d];
-        bad = bad || !isfinite((double)f[d]);
-      }
-      acc[0] = m;
-      acc[1] = bad ? 1.0 : 0.0;
-      has = true;
-    }
-  }
-  block_force_reduce(acc, has, out);
-}
-
-// ---- initial state ------------------------------------------------------------------------
-template <class SP>
-__global__ void aa_init_kernel(const InitParams p, typename SP::S* __restrict__ A,
-                               const uint8_t* __restrict__ flags) {
-  using C = typename SP::C;
-  const Grid& g = p.g;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny) return;
-  const long long i = node_index(g, x, y, z);
-  const C rho0 = C(p.rho0);
-  const bool solid = (flags[i] & F_SOLID) != 0;
-  if (p.f_in) {
-#pragma unroll
-    for (int d = 0; d < Q; d++) SP::st(A + (long long)d * g.plane + i, C(import_value(p, g, i, d)), d, rho0);
-    return;
-  }
-  const C r = p.rho ? C(p.rho[i]) : rho0;
-  const C u = p.u ? C(p.u[i]) : C(p.uni[0]);
-  const C v = p.v ? C(p.v[i]) : C(p.uni[1]);
-  const C w = p.w ? C(p.w[i]) : C(p.uni[2]);
-#pragma unroll
-  for (int d = 0; d < Q; d++)
-    SP::st(A + (long long)d * g.plane + i, solid ? C(0) : feq<C>(d, r, u, v, w), d, rho0);
-}
-
-// ---- host launchers ------------------------------------------------------------------------
-template <class SP, bool ODD, bool TRT, bool FORCE>
-static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, dim3 grid, dim3 block,
-                              cudaStream_t s) {
-  if (p.tma.enabled) {
-    auto kern = aa_tma_kernel<SP, ODD, TRT, FORCE>;
-    const int smem = p.tma.stages * p.tma.stage_bytes;
-    static thread_local int configured_smem = -1;  // per instantiation
-    if (configured_smem != smem) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      if (e != cudaSuccess) return e;
-      configured_smem = smem;
-    }
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p.tma.tw, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    long long nb = (long long)sms * per_sm;
-    if (nb > p.tma.ntiles) nb = p.tma.ntiles;
-    kern<<<(unsigned)nb, p.tma.tw, smem, s>>>(p, (typename SP::S*)A, flags);
-    return cudaGetLastError();
-  }
-  aa_step_kernel<SP, ODD, TRT, FORCE><<<grid, block, 0, s>>>(p, (typename SP::S*)A, flags);
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 // Per-tile boundary bits: 1 = the even phase needs the direct path, 2 = the odd
@@ -874,76 +107,13 @@ cudaError_t aa_launch_tile_flags(const Grid& g, int tw, long long ntiles, const 
   return cudaGetLastError();
 }
 
-template <class SP>
-static cudaError_t launch_sp(const AAParams& p, void* A, const uint8_t* flags, bool odd, bool trt,
-                             bool force, dim3 grid, dim3 block, cudaStream_t s) {
-#define LBM_AA_CASE(O, T, F)                                                  \
-  if (odd == O && trt == T && force == F)                                     \
-    return launch_one<SP, O, T, F>(p, A, flags, grid, block, s);
-  LBM_AA_CASE(false, false, false)
-  LBM_AA_CASE(false, false, true)
-  LBM_AA_CASE(false, true, false)
-  LBM_AA_CASE(false, true, true)
-  LBM_AA_CASE(true, false, false)
-  LBM_AA_CASE(true, false, true)
-  LBM_AA_CASE(true, true, false)
-  LBM_AA_CASE(true, true, true)
-#undef LBM_AA_CASE
-  return cudaErrorInvalidValue;
+// One thread advances the batch step counter (read by the next batched step).
+__global__ void batch_advance_kernel(long long* counter) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *counter += 1;
 }
 
-cudaError_t aa_launch_step(int storage, const AAParams& p, void* A, const uint8_t* flags, bool odd,
-                           bool trt, bool force, dim3 grid, dim3 block, cudaStream_t s) {
-  switch (storage) {
-    case LBM_STORE_FP32: return launch_sp<StF32>(p, A, flags, odd, trt, force, grid, block, s);
-    case LBM_STORE_FP64: return launch_sp<StF64>(p, A, flags, odd, trt, force, grid, block, s);
-    case LBM_STORE_FP16DEV: return launch_sp<StF16>(p, A, flags, odd, trt, force, grid, block, s);
-  }
-  return cudaErrorInvalidValue;
-}
-
-cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
-                             const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s) {
-  switch (storage) {
-    case LBM_STORE_FP32:
-      aa_export_kernel<StF32><<<grid, block, 0, s>>>(p, (const float*)A, flags, out);
-      break;
-    case LBM_STORE_FP64:
-      aa_export_kernel<StF64><<<grid, block, 0, s>>>(p, (const double*)A, flags, out);
-      break;
-    case LBM_STORE_FP16DEV:
-      aa_export_kernel<StF16><<<grid, block, 0, s>>>(p, (const __half*)A, flags, out);
-      break;
-    default: return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
-                             double* out, dim3 grid, dim3 block, cudaStream_t s) {
-  switch (storage) {
-    case LBM_STORE_FP32:
-      aa_reduce_kernel<StF32><<<grid, block, 0, s>>>(p, (const float*)A, flags, out);
-      break;
-    case LBM_STORE_FP64:
-      aa_reduce_kernel<StF64><<<grid, block, 0, s>>>(p, (const double*)A, flags, out);
-      break;
-    case LBM_STORE_FP16DEV:
-      aa_reduce_kernel<StF16><<<grid, block, 0, s>>>(p, (const __half*)A, flags, out);
-      break;
-    default: return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t aa_launch_init(int storage, const InitParams& p, void* A, const uint8_t* flags, dim3 grid,
-                           dim3 block, cudaStream_t s) {
-  switch (storage) {
-    case LBM_STORE_FP32: aa_init_kernel<StF32><<<grid, block, 0, s>>>(p, (float*)A, flags); break;
-    case LBM_STORE_FP64: aa_init_kernel<StF64><<<grid, block, 0, s>>>(p, (double*)A, flags); break;
-    case LBM_STORE_FP16DEV: aa_init_kernel<StF16><<<grid, block, 0, s>>>(p, (__half*)A, flags); break;
-    default: return cudaErrorInvalidValue;
-  }
+cudaError_t aa_launch_batch_advance(long long* counter, cudaStream_t s) {
+  batch_advance_kernel<<<1, 32, 0, s>>>(counter);
   return cudaGetLastError();
 }
 

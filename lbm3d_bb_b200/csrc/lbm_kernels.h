@@ -40,6 +40,27 @@ struct AAParams {
   const unsigned long long* links;
 };
 
+// Batched step over many independent config-mode domains (one launch per step).
+constexpr int BATCH_ITEM = 128;  // cells per work item = threads per block
+
+struct BatchDom {
+  AAParams p[2];         // parameter blocks of the even [0] and odd [1] phase
+  void* A;               // populations
+  const uint8_t* flags;
+  double* ring;          // force records (ring_slots x FORCE_RECORD doubles)
+  int ring_slots;
+  int phase0;            // phase of batch step 0 (0 even, 1 odd)
+  long long base_step;   // steps the domain had completed before batch step 0
+  long long item_begin;  // first work item of the domain
+};
+
+struct BatchParams {
+  const BatchDom* doms;
+  const int* item_dom;       // domain of every work item
+  long long items;           // work items in total
+  const long long* counter;  // batch steps completed (advanced on the device)
+};
+
 // Reference-mode step (two population buffers, virtual-fluid solids).
 struct RefParams {
   Grid g;
@@ -176,9 +197,15 @@ __device__ __forceinline__ void block_force_reduce(double* acc, bool has, double
   }
 }
 
-// ---- launchers (kernels_aa.cu) ----
+// ---- launchers (kernels_aa.cu; kernels in aa_impl.cuh) ----
+// faces: some axis is not periodic (selects the kernel that keeps face nodes on the
+// fast path; the other kernel sends them to the general path).
 cudaError_t aa_launch_step(int storage, const AAParams& p, void* A, const uint8_t* flags, bool odd,
-                           bool trt, bool force, dim3 grid, dim3 block, cudaStream_t s);
+                           bool trt, bool force, bool faces, dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t aa_launch_batch(int storage, const BatchParams& bp, bool trt, bool force, bool faces, int blocks,
+                            cudaStream_t s);
+cudaError_t aa_batch_blocks_per_sm(int storage, bool trt, bool force, bool faces, int* per_sm);
+cudaError_t aa_launch_batch_advance(long long* counter, cudaStream_t s);
 cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
                              const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags,

@@ -697,6 +697,12 @@ struct Sim {
                 case LBM_FACE_OUTFLOW:
                   val = P[d * N + i];
                   break;
+                case LBM_FACE_PRESSURE: {  // anti-bounce-back at rho0 with the node's velocity
+                  T cu = T(CX[d]) * uN[i] + T(CY[d]) * vN[i] + T(CZ[d]) * wN[i];
+                  T usq = uN[i] * uN[i] + vN[i] * vN[i] + wN[i] * wN[i];
+                  val = -P[o * N + i] + T(2) * w[d] * T(cfg.rho0) * (T(1) + T(4.5) * cu * cu - T(1.5) * usq);
+                  break;
+                }
                 default: {  // WALL: half-way bounce-back with wall velocity
                   T cdu = T(CX[o]) * T(fu[0]) + T(CY[o]) * T(fu[1]) + T(CZ[o]) * T(fu[2]);
                   val = P[o * N + i] - T(6) * w[o] * rN[i] * cdu;

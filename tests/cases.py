@@ -15,10 +15,11 @@ def face_u_inlet(u):
     return [(u, 0.0, 0.0)] + [(0.0, 0.0, 0.0)] * 5
 
 
-def sphere_channel(cls, nx=48, ny=24, nz=24, r=4.0, center=None, tau=0.8, u_in=0.04, storage="fp64", **kw):
+def sphere_channel(cls, nx=48, ny=24, nz=24, r=4.0, center=None, tau=0.8, u_in=0.04, storage="fp64",
+                   faces=INLET_CHANNEL, **kw):
     """C1 in miniature: fixed sphere, equilibrium inlet, zero-gradient outlet, no-slip walls."""
     center = center or (nx / 4, ny / 2, nz / 2)
-    d = cls(nx, ny, nz, collision="BGK", storage=storage, faces=INLET_CHANNEL, omega_p=1.0 / tau,
+    d = cls(nx, ny, nz, collision="BGK", storage=storage, faces=faces, omega_p=1.0 / tau,
             face_u=face_u_inlet(u_in), **kw)
     d.add_sphere(center, r)
     d.init_equilibrium()

@@ -48,6 +48,21 @@ def test_sphere_channel_fp64(gpu, oracle_lib, steps):
     assert abs(g.mass() - o.mass()) <= 1e-10 * abs(o.mass())
 
 
+@pytest.mark.parametrize("outlet", ["pressure", "outflow"])
+@pytest.mark.parametrize("storage_steps", [1, 2, 33])
+def test_channel_outlets_fp64(gpu, oracle_lib, outlet, storage_steps):
+    """Face nodes on the fast path (odd-sized box, non-periodic faces) against the oracle."""
+    faces = ("inlet", outlet, "wall", "wall", "wall", "wall")
+    kw = dict(nx=37, ny=19, nz=13, r=3.5, center=(12.2, 9.6, 6.4), u_in=0.05, faces=faces)
+    g = cases.sphere_channel(Domain, **kw)
+    o = cases.sphere_channel(OracleDomain, **kw)
+    g.step(storage_steps)
+    o.step(storage_steps)
+    assert rel_l2(g.populations(), o.populations()) <= 1e-12
+    _macros_close(g, o, TOL_FIELD)
+    _force_close(g.force_history(1, storage_steps)[:, :3], o.force_history(1, storage_steps)[:, :3], TOL_FORCE)
+
+
 def test_sphere_channel_flags_links(gpu, oracle_lib):
     g = cases.sphere_channel(Domain)
     o = cases.sphere_channel(OracleDomain)
