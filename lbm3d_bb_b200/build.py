@@ -18,6 +18,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 LIB = PKG / "liblbm3d.so"
+UNET_LIB = PKG / "libunet3d.so"
 OBJ = PKG / "_build"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -74,7 +75,21 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_unet(verbose, force)
     return LIB
+
+
+def build_unet(verbose: bool = False, force: bool = False) -> Path:
+    """libunet3d.so: the warm-start network's kernels (separate C ABI, include/unet3d.h)."""
+    OBJ.mkdir(exist_ok=True)
+    src = CSRC / "unet3d.cu"
+    if force or _stale(UNET_LIB, [src, INCLUDE / "unet3d.h"]):
+        cmd = [nvcc(), *ARCH, *COMMON, "-shared", str(src), "-o", str(UNET_LIB), "-lcudart"]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return UNET_LIB
 
 
 if __name__ == "__main__":

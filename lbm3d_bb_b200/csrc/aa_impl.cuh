@@ -624,6 +624,21 @@ __global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __gr
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
+// q = n / d and r = n % d for n < 2^31 through an FP64 reciprocal (exact after the
+// one-step correction; the product is off by at most one).
+__device__ __forceinline__ void divmod_rcp(const unsigned n, const int d, const double inv, unsigned& q, int& r) {
+  q = (unsigned)((double)n * inv);
+  r = (int)(n - q * (unsigned)d);
+  if (r < 0) {
+    q--;
+    r += d;
+  } else if (r >= d) {
+    q++;
+    r -= d;
+  }
+}
+
+
 // ---- batched persistent step over many domains -------------------------------------
 // Work items are runs of BATCH_ITEM consecutive cells of one domain; every domain's
 // items are numbered consecutively and item_dom maps an item to its domain.  Each
@@ -645,9 +660,20 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
   const uint8_t* flags = nullptr;
   double* rec = nullptr;
   long long item0 = 0;
+  double inv_nx = 0.0, inv_ny = 0.0;
+  // force / torque of the current domain, reduced once per domain and block
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  const int stripe = (int)(blockIdx.x % FORCE_SLOTS) * 8;
   for (long long item = first; item < last; item++) {
     const int d = bp.item_dom[item];
     if (d != dom) {
+      if (dom >= 0 && sp.compute_force) {
+        block_force_reduce(acc, has_link, rec + stripe);
+#pragma unroll
+        for (int c = 0; c < 6; c++) acc[c] = 0.0;
+        has_link = false;
+      }
       __syncthreads();  // every thread is done with the previous parameter block
       dom = d;
       const BatchDom& D = bp.doms[d];
@@ -665,24 +691,24 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
         for (int w = t; w < FORCE_RECORD; w += BATCH_ITEM) next[w] = 0.0;
       }
       __syncthreads();
+      inv_nx = 1.0 / (double)sp.g.nx;
+      inv_ny = 1.0 / (double)sp.g.ny;
     }
     const Grid& g = sp.g;
     // a domain holds fewer than 2^31 cells: 32-bit index arithmetic
     const unsigned cell = (unsigned)(item - item0) * BATCH_ITEM + t;
     const bool inb = cell < (unsigned)g.N;
-    const unsigned row = cell / (unsigned)g.nx;
-    const int x = (int)(cell - row * (unsigned)g.nx);
-    const int y = (int)(row % (unsigned)g.ny), z = (int)(row / (unsigned)g.ny);
-    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    bool has_link = false;
+    unsigned row, z;
+    int x, y;
+    divmod_rcp(cell, g.nx, inv_nx, row, x);
+    divmod_rcp(row, g.ny, inv_ny, z, y);
     if (phase)
-      aa_direct<SP, true, TRT, FORCE, FACES>(sp, A, flags, x, y, z, inb, acc, &has_link);
+      aa_direct<SP, true, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
     else
-      aa_direct<SP, false, TRT, FORCE, FACES>(sp, A, flags, x, y, z, inb, acc, &has_link);
-    if (sp.compute_force) block_force_reduce(acc, has_link, rec + (int)(item % FORCE_SLOTS) * 8);
+      aa_direct<SP, false, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
   }
+  if (dom >= 0 && sp.compute_force) block_force_reduce(acc, has_link, rec + stripe);
 }
-
 
 // ---- TMA-staged persistent step ------------------------------------------------------
 // Tiles are row segments of TW cells.  For every tile without a boundary node, one

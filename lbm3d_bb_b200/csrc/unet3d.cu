@@ -1,0 +1,571 @@
+// unet3d.cu — kernels of the learned warm start (include/unet3d.h): 3x3x3
+// convolutions as implicit GEMMs on the BF16 tensor cores (mma.sync m16n8k16,
+// FP32 accumulation), their data and weight gradients, 2x pooling / upsampling with
+// skip concatenation, the masked MSE loss and Adam.
+//
+// Forward (and data-gradient) convolution: one warp computes a tile of 16
+// consecutive voxels along x by all output channels.  The K loop runs over the 27
+// taps and 16-channel slices of the input; A fragments are read straight from the
+// channels-last activations (each thread loads the 32-bit channel pairs of two
+// voxels), B fragments from the [tap][Cout][Cin] weights, both through the read-only
+// cache.  Taps whose row lies outside the box are skipped warp-uniformly; voxels
+// outside the row read zero.
+//
+// Weight gradient: dW[tap] = dY^T X_shift is a GEMM whose reduction runs over the
+// voxels.  A block owns one tap, a 16-channel input slice and a chunk of voxels:
+// it stages 64-voxel slabs of dY and of the shifted input in shared memory and
+// feeds the MMAs with transposing ldmatrix loads; partial sums go to the FP32
+// gradient with one atomic add per element and block.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/unet3d.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return 1;
+}
+
+int launched(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail("%s: %s", what, cudaGetErrorString(e));
+  return 0;
+}
+
+using bf16 = __nv_bfloat16;
+
+struct Geo {
+  int n, d, h, w;
+};
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t* r, const void* smem_row) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem_row);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// ---- forward convolution ------------------------------------------------------------
+template <int NT>  // output channels / 8
+__global__ void __launch_bounds__(128) conv_fwd_kernel(const bf16* __restrict__ in, const bf16* __restrict__ w,
+                                                       const float* __restrict__ bias, bf16* __restrict__ out,
+                                                       const Geo g, const int cin, const int relu,
+                                                       const long long tiles) {
+  const int lane = threadIdx.x & 31;
+  const long long tile = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (tile >= tiles) return;  // whole warp
+  const int tpr = g.w / 16;
+  long long row = tile / tpr;
+  const int x0 = (int)(tile - row * tpr) * 16;
+  const int y = (int)(row % g.h);
+  row /= g.h;
+  const int z = (int)(row % g.d);
+  const int n = (int)(row / g.d);
+  const int gid = lane >> 2, tig = lane & 3;
+  constexpr int COUT = NT * 8;
+  const int cw = cin / 2;  // 32-bit words per voxel
+  const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+  const uint32_t* w32 = reinterpret_cast<const uint32_t*>(w);
+  float acc[NT][4];
+#pragma unroll
+  for (int t = 0; t < NT; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
+  for (int dz = -1; dz <= 1; dz++) {
+    const int zz = z + dz;
+    if (zz < 0 || zz >= g.d) continue;
+    for (int dy = -1; dy <= 1; dy++) {
+      const int yy = y + dy;
+      if (yy < 0 || yy >= g.h) continue;
+      const long long rbase = (((long long)n * g.d + zz) * g.h + yy) * g.w;
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++) {
+        const int tap = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+        const int xa = x0 + gid + dx, xb = xa + 8;
+        const bool va = xa >= 0 && xa < g.w, vb = xb >= 0 && xb < g.w;
+        const uint32_t* pa = in32 + (rbase + (va ? xa : 0)) * cw + tig;
+        const uint32_t* pb = in32 + (rbase + (vb ? xb : 0)) * cw + tig;
+        const uint32_t* wt = w32 + ((long long)tap * COUT + gid) * cw + tig;
+        for (int k2 = 0; k2 < cw; k2 += 8) {
+          uint32_t a[4];
+          a[0] = va ? __ldg(pa + k2) : 0u;
+          a[1] = vb ? __ldg(pb + k2) : 0u;
+          a[2] = va ? __ldg(pa + k2 + 4) : 0u;
+          a[3] = vb ? __ldg(pb + k2 + 4) : 0u;
+#pragma unroll
+          for (int t = 0; t < NT; t++) {
+            const uint32_t* wb = wt + (long long)t * 8 * cw + k2;
+            const uint32_t b[2] = {__ldg(wb), __ldg(wb + 4)};
+            mma_bf16(acc[t], a, b);
+          }
+        }
+      }
+    }
+  }
+  const long long vbase = (((long long)n * g.d + z) * g.h + y) * g.w + x0;
+  uint32_t* o32 = reinterpret_cast<uint32_t*>(out);
+#pragma unroll
+  for (int t = 0; t < NT; t++) {
+    const int co = t * 8 + 2 * tig;
+    const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
+    float v0 = acc[t][0] + b0, v1 = acc[t][1] + b1, v2 = acc[t][2] + b0, v3 = acc[t][3] + b1;
+    if (relu) {
+      v0 = fmaxf(v0, 0.f);
+      v1 = fmaxf(v1, 0.f);
+      v2 = fmaxf(v2, 0.f);
+      v3 = fmaxf(v3, 0.f);
+    }
+    o32[((vbase + gid) * COUT + co) / 2] = pack_bf16(v0, v1);
+    o32[((vbase + gid + 8) * COUT + co) / 2] = pack_bf16(v2, v3);
+  }
+}
+
+// wt[26 - tap][ci][co] = w[tap][co][ci]
+__global__ void flip_kernel(const bf16* __restrict__ w, bf16* __restrict__ wt, int cin, int cout) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int total = 27 * cin * cout;
+  if (i >= total) return;
+  const int ci = i % cin, co = (i / cin) % cout, tap = i / (cin * cout);
+  wt[((26 - tap) * cin + ci) * cout + co] = w[i];
+}
+
+// ---- weight gradient ----------------------------------------------------------------
+constexpr int BW_KV = 64;  // voxels per shared-memory slab
+
+template <int CB>  // output channels / 16 (1, 2 or 4)
+__global__ void __launch_bounds__(128) conv_bwdw_kernel(const bf16* __restrict__ in, const bf16* __restrict__ dout,
+                                                        float* __restrict__ dw, const Geo g, const int cin,
+                                                        const long long vox, const long long chunk) {
+  constexpr int COUT = CB * 16;
+  constexpr int SA = COUT + 8, SB = 16 + 8;  // padded row lengths (16-byte multiples)
+  __shared__ __align__(16) bf16 sA[BW_KV * SA];
+  __shared__ __align__(16) bf16 sB[BW_KV * SB];
+  const int tap = blockIdx.z;
+  const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+  const int ci0 = blockIdx.y * 16;
+  const long long m_begin = (long long)blockIdx.x * chunk;
+  const long long m_end = m_begin + chunk < vox ? m_begin + chunk : vox;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int NWB = CB < 4 ? CB : 4;  // warps sharing the output-channel blocks
+  const int cb = warp % NWB, phase = warp / NWB, nphase = 4 / NWB;
+  float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (long long m0 = m_begin; m0 < m_end; m0 += BW_KV) {
+    // dY slab: BW_KV voxels x COUT channels, 16-byte chunks
+    for (int c = tid; c < BW_KV * (COUT / 8); c += 128) {
+      const int i = c / (COUT / 8), part = c % (COUT / 8);
+      const long long m = m0 + i;
+      const uint4 v = m < m_end ? *reinterpret_cast<const uint4*>(dout + m * COUT + part * 8) : zero;
+      *reinterpret_cast<uint4*>(sA + i * SA + part * 8) = v;
+    }
+    // shifted input slab: BW_KV voxels x 16 channels
+    {
+      const int i = tid >> 1, part = tid & 1;
+      const long long m = m0 + i;
+      uint4 v = zero;
+      if (m < m_end) {
+        long long t = m;
+        const int x = (int)(t % g.w);
+        t /= g.w;
+        const int y = (int)(t % g.h);
+        t /= g.h;
+        const int z = (int)(t % g.d);
+        const int xx = x + dx, yy = y + dy, zz = z + dz;
+        if (xx >= 0 && xx < g.w && yy >= 0 && yy < g.h && zz >= 0 && zz < g.d) {
+          const long long nb = m + dx + (long long)g.w * (dy + (long long)g.h * dz);
+          v = *reinterpret_cast<const uint4*>(in + nb * cin + ci0 + part * 8);
+        }
+      }
+      *reinterpret_cast<uint4*>(sB + i * SB + part * 8) = v;
+    }
+    __syncthreads();
+    for (int k16 = phase; k16 < BW_KV / 16; k16 += nphase) {
+      const int i = lane & 7, mat = lane >> 3;
+      uint32_t a[4], b[4];
+      ldsm_x4_trans(a, sA + (k16 * 16 + i + (mat >= 2 ? 8 : 0)) * SA + cb * 16 + ((mat & 1) ? 8 : 0));
+      ldsm_x4_trans(b, sB + (k16 * 16 + i + ((mat & 1) ? 8 : 0)) * SB + (mat >> 1) * 8);
+      mma_bf16(acc[0], a, b);
+      mma_bf16(acc[1], a, b + 2);
+    }
+    __syncthreads();
+  }
+  const int gid = lane >> 2, tig = lane & 3;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int co = cb * 16 + gid, ci = ci0 + t * 8 + 2 * tig;
+    float* p = dw + ((long long)tap * COUT + co) * cin + ci;
+    atomicAdd(p, acc[t][0]);
+    atomicAdd(p + 1, acc[t][1]);
+    atomicAdd(p + 8LL * cin, acc[t][2]);
+    atomicAdd(p + 8LL * cin + 1, acc[t][3]);
+  }
+}
+
+__global__ void bias_grad_kernel(const bf16* __restrict__ dout, float* __restrict__ db, long long voxels, int c) {
+  extern __shared__ float sacc[];
+  for (int k = threadIdx.x; k < c; k += blockDim.x) sacc[k] = 0.f;
+  __syncthreads();
+  const long long total = voxels * c;
+  float s = 0.f;
+  // the stride is a multiple of c, so each thread keeps one channel; threads past
+  // the stride would repeat elements and stay idle
+  const long long stride = (long long)gridDim.x * blockDim.x / c * c;
+  const long long start = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (start < stride) {
+    for (long long i = start; i < total; i += stride) s += __bfloat162float(dout[i]);
+    atomicAdd(&sacc[start % c], s);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < c; k += blockDim.x) atomicAdd(db + k, sacc[k]);
+}
+
+__global__ void relu_bwd_kernel(bf16* __restrict__ dy, const bf16* __restrict__ y, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count && !(__bfloat162float(y[i]) > 0.f)) dy[i] = __float2bfloat16(0.f);
+}
+
+// ---- pooling, upsampling, concatenation ---------------------------------------------
+__global__ void pool2_kernel(const bf16* __restrict__ in, bf16* __restrict__ out, Geo f, int c, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;  // count = coarse elements
+  const int ch = (int)(i % c);
+  long long t = i / c;
+  const int W = f.w / 2, H = f.h / 2, D = f.d / 2;
+  const int x = (int)(t % W);
+  t /= W;
+  const int y = (int)(t % H);
+  t /= H;
+  const int z = (int)(t % D);
+  const int n = (int)(t / D);
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const long long v = (((long long)n * f.d + 2 * z + (k >> 2)) * f.h + 2 * y + ((k >> 1) & 1)) * f.w + 2 * x + (k & 1);
+    s += __bfloat162float(in[v * c + ch]);
+  }
+  out[i] = __float2bfloat16(s * 0.125f);
+}
+
+__global__ void pool2_bwd_kernel(const bf16* __restrict__ dout, bf16* __restrict__ din, Geo f, int c, int accumulate,
+                                 long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;  // count = fine elements
+  const int ch = (int)(i % c);
+  long long t = i / c;
+  const int x = (int)(t % f.w);
+  t /= f.w;
+  const int y = (int)(t % f.h);
+  t /= f.h;
+  const int z = (int)(t % f.d);
+  const int n = (int)(t / f.d);
+  const long long p = (((long long)n * (f.d / 2) + z / 2) * (f.h / 2) + y / 2) * (f.w / 2) + x / 2;
+  float v = __bfloat162float(dout[p * c + ch]) * 0.125f;
+  if (accumulate) v += __bfloat162float(din[i]);
+  din[i] = __float2bfloat16(v);
+}
+
+__global__ void up2_concat_kernel(const bf16* __restrict__ low, const bf16* __restrict__ skip, bf16* __restrict__ out,
+                                  Geo f, int cu, int cs, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;  // count = fine voxels * (cu + cs)
+  const int ct = cu + cs;
+  const int ch = (int)(i % ct);
+  const long long v = i / ct;
+  if (ch >= cu) {
+    out[i] = skip[v * cs + (ch - cu)];
+    return;
+  }
+  long long t = v;
+  const int x = (int)(t % f.w);
+  t /= f.w;
+  const int y = (int)(t % f.h);
+  t /= f.h;
+  const int z = (int)(t % f.d);
+  const int n = (int)(t / f.d);
+  const long long p = (((long long)n * (f.d / 2) + z / 2) * (f.h / 2) + y / 2) * (f.w / 2) + x / 2;
+  out[i] = low[p * cu + ch];
+}
+
+__global__ void up2_concat_bwd_low_kernel(const bf16* __restrict__ dcat, bf16* __restrict__ dlow, Geo f, int cu, int cs,
+                                          long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;  // count = coarse voxels * cu
+  const int ch = (int)(i % cu);
+  long long t = i / cu;
+  const int W = f.w / 2, H = f.h / 2, D = f.d / 2;
+  const int x = (int)(t % W);
+  t /= W;
+  const int y = (int)(t % H);
+  t /= H;
+  const int z = (int)(t % D);
+  const int n = (int)(t / D);
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const long long v = (((long long)n * f.d + 2 * z + (k >> 2)) * f.h + 2 * y + ((k >> 1) & 1)) * f.w + 2 * x + (k & 1);
+    s += __bfloat162float(dcat[v * (cu + cs) + ch]);
+  }
+  dlow[i] = __float2bfloat16(s);
+}
+
+__global__ void up2_concat_bwd_skip_kernel(const bf16* __restrict__ dcat, bf16* __restrict__ dskip, int cu, int cs,
+                                           long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;  // count = fine voxels * cs
+  const long long v = i / cs;
+  dskip[i] = dcat[v * (cu + cs) + cu + (int)(i % cs)];
+}
+
+// ---- loss and optimiser -------------------------------------------------------------
+__global__ void mse_kernel(const bf16* __restrict__ out, const float* __restrict__ target,
+                           const uint8_t* __restrict__ mask, const float* __restrict__ cw, bf16* __restrict__ dout,
+                           double* loss, long long voxels, int cpad, int ct, double count) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double l = 0.0;
+  if (v < voxels) {
+    const bool on = mask[v] != 0;
+    for (int c = 0; c < cpad; c++) {
+      float gr = 0.f;
+      if (on && c < ct) {
+        const float d = __bfloat162float(out[v * cpad + c]) - target[v * ct + c];
+        l += (double)cw[c] * d * d;
+        gr = (float)(2.0 * cw[c] * d / count);
+      }
+      dout[v * cpad + c] = __float2bfloat16(gr);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+  if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss, l / count);
+}
+
+__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, bf16* __restrict__ wb, long long count, float lr, float b1, float b2,
+                            float eps, float c1, float c2) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16(wi);
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ x, bf16* __restrict__ y, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) y[i] = __float2bfloat16(x[i]);
+}
+
+__global__ void from_bf16_kernel(const bf16* __restrict__ x, float* __restrict__ y, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) y[i] = __bfloat162float(x[i]);
+}
+
+// out[0] += sum (a - b)^2, out[1] += sum a^2 (FP64), for steady-state tests.
+__global__ void diff_norms_kernel(const float* __restrict__ a, const float* __restrict__ b, long long count,
+                                  double* out) {
+  double d2 = 0.0, a2 = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x) {
+    const double x = a[i], y = b[i];
+    d2 += (x - y) * (x - y);
+    a2 += x * x;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d2 += __shfl_down_sync(0xffffffffu, d2, o);
+    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, d2);
+    atomicAdd(out + 1, a2);
+  }
+}
+
+unsigned blocks_for(long long count, int per) { return (unsigned)((count + per - 1) / per); }
+
+bool geo_ok(int n, int d, int h, int w) { return n > 0 && d > 0 && h > 0 && w > 0; }
+
+}  // namespace
+
+extern "C" {
+
+int32_t nn_abi_version(void) { return UNET3D_ABI_VERSION; }
+
+const char* nn_last_error(void) { return g_err.c_str(); }
+
+int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* out, int32_t n, int32_t d, int32_t h,
+                      int32_t wd, int32_t cin, int32_t cout, int32_t relu, void* stream) {
+  if (!in || !w || !out || !geo_ok(n, d, h, wd)) return fail("nn_conv3d_fwd: null pointer or empty shape");
+  if (wd % 16 || cin % 16 || cin <= 0) return fail("nn_conv3d_fwd: W (%d) and Cin (%d) must be multiples of 16", wd, cin);
+  const Geo g{n, d, h, wd};
+  const long long tiles = (long long)n * d * h * (wd / 16);
+  const unsigned grid = blocks_for(tiles, 4);
+  cudaStream_t s = (cudaStream_t)stream;
+  const bf16* I = (const bf16*)in;
+  const bf16* W = (const bf16*)w;
+  bf16* O = (bf16*)out;
+  switch (cout) {
+    case 16: conv_fwd_kernel<2><<<grid, 128, 0, s>>>(I, W, bias, O, g, cin, relu, tiles); break;
+    case 32: conv_fwd_kernel<4><<<grid, 128, 0, s>>>(I, W, bias, O, g, cin, relu, tiles); break;
+    case 48: conv_fwd_kernel<6><<<grid, 128, 0, s>>>(I, W, bias, O, g, cin, relu, tiles); break;
+    case 64: conv_fwd_kernel<8><<<grid, 128, 0, s>>>(I, W, bias, O, g, cin, relu, tiles); break;
+    case 96: conv_fwd_kernel<12><<<grid, 128, 0, s>>>(I, W, bias, O, g, cin, relu, tiles); break;
+    default: return fail("nn_conv3d_fwd: Cout %d not in {16, 32, 48, 64, 96}", cout);
+  }
+  return launched("nn_conv3d_fwd");
+}
+
+int32_t nn_conv3d_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream) {
+  if (!w || !wt || cin <= 0 || cout <= 0) return fail("nn_conv3d_flip: bad arguments");
+  const int total = 27 * cin * cout;
+  flip_kernel<<<blocks_for(total, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)w, (bf16*)wt, cin, cout);
+  return launched("nn_conv3d_flip");
+}
+
+int32_t nn_conv3d_bwd_weight(const void* in, const void* dout, float* dw, int32_t n, int32_t d, int32_t h, int32_t wd,
+                             int32_t cin, int32_t cout, void* stream) {
+  if (!in || !dout || !dw || !geo_ok(n, d, h, wd)) return fail("nn_conv3d_bwd_weight: null pointer or empty shape");
+  if (cin % 16 || cin <= 0) return fail("nn_conv3d_bwd_weight: Cin %d must be a multiple of 16", cin);
+  const long long vox = (long long)n * d * h * wd;
+  const long long chunk = 4096;
+  dim3 grid(blocks_for(vox, (int)chunk), (unsigned)(cin / 16), 27);
+  const Geo g{n, d, h, wd};
+  cudaStream_t s = (cudaStream_t)stream;
+  const bf16* I = (const bf16*)in;
+  const bf16* D = (const bf16*)dout;
+  switch (cout) {
+    case 16: conv_bwdw_kernel<1><<<grid, 128, 0, s>>>(I, D, dw, g, cin, vox, chunk); break;
+    case 32: conv_bwdw_kernel<2><<<grid, 128, 0, s>>>(I, D, dw, g, cin, vox, chunk); break;
+    case 64: conv_bwdw_kernel<4><<<grid, 128, 0, s>>>(I, D, dw, g, cin, vox, chunk); break;
+    default: return fail("nn_conv3d_bwd_weight: Cout %d not in {16, 32, 64}", cout);
+  }
+  return launched("nn_conv3d_bwd_weight");
+}
+
+int32_t nn_bias_grad(const void* dout, float* db, int64_t voxels, int32_t c, void* stream) {
+  if (!dout || !db || voxels <= 0 || c <= 0 || c > 256) return fail("nn_bias_grad: bad arguments");
+  const long long total = voxels * c;
+  unsigned grid = blocks_for(total, 256 * 16);
+  if (grid > 4096) grid = 4096;
+  bias_grad_kernel<<<grid, 256, c * sizeof(float), (cudaStream_t)stream>>>((const bf16*)dout, db, voxels, c);
+  return launched("nn_bias_grad");
+}
+
+int32_t nn_relu_bwd(void* dy, const void* y, int64_t count, void* stream) {
+  if (!dy || !y || count < 0) return fail("nn_relu_bwd: bad arguments");
+  if (count == 0) return 0;
+  relu_bwd_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>((bf16*)dy, (const bf16*)y, count);
+  return launched("nn_relu_bwd");
+}
+
+int32_t nn_pool2(const void* in, void* out, int32_t n, int32_t d, int32_t h, int32_t wd, int32_t c, void* stream) {
+  if (!in || !out || !geo_ok(n, d, h, wd) || c <= 0 || d % 2 || h % 2 || wd % 2) return fail("nn_pool2: bad shape");
+  const long long count = (long long)n * (d / 2) * (h / 2) * (wd / 2) * c;
+  pool2_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)in, (bf16*)out,
+                                                                          Geo{n, d, h, wd}, c, count);
+  return launched("nn_pool2");
+}
+
+int32_t nn_pool2_bwd(const void* dout, void* din, int32_t n, int32_t d, int32_t h, int32_t wd, int32_t c,
+                     int32_t accumulate, void* stream) {
+  if (!dout || !din || !geo_ok(n, d, h, wd) || c <= 0 || d % 2 || h % 2 || wd % 2) return fail("nn_pool2_bwd: bad shape");
+  const long long count = (long long)n * d * h * wd * c;
+  pool2_bwd_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)dout, (bf16*)din,
+                                                                              Geo{n, d, h, wd}, c, accumulate, count);
+  return launched("nn_pool2_bwd");
+}
+
+int32_t nn_up2_concat(const void* low, const void* skip, void* out, int32_t n, int32_t d, int32_t h, int32_t wd,
+                      int32_t cu, int32_t cs, void* stream) {
+  if (!low || !skip || !out || !geo_ok(n, d, h, wd) || cu <= 0 || cs <= 0 || d % 2 || h % 2 || wd % 2)
+    return fail("nn_up2_concat: bad shape");
+  const long long count = (long long)n * d * h * wd * (cu + cs);
+  up2_concat_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>(
+      (const bf16*)low, (const bf16*)skip, (bf16*)out, Geo{n, d, h, wd}, cu, cs, count);
+  return launched("nn_up2_concat");
+}
+
+int32_t nn_up2_concat_bwd(const void* dcat, void* dlow, void* dskip, int32_t n, int32_t d, int32_t h, int32_t wd,
+                          int32_t cu, int32_t cs, void* stream) {
+  if (!dcat || !dlow || !dskip || !geo_ok(n, d, h, wd) || cu <= 0 || cs <= 0 || d % 2 || h % 2 || wd % 2)
+    return fail("nn_up2_concat_bwd: bad shape");
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long cl = (long long)n * (d / 2) * (h / 2) * (wd / 2) * cu;
+  up2_concat_bwd_low_kernel<<<blocks_for(cl, 256), 256, 0, s>>>((const bf16*)dcat, (bf16*)dlow, Geo{n, d, h, wd}, cu,
+                                                                 cs, cl);
+  const long long cf = (long long)n * d * h * wd * cs;
+  up2_concat_bwd_skip_kernel<<<blocks_for(cf, 256), 256, 0, s>>>((const bf16*)dcat, (bf16*)dskip, cu, cs, cf);
+  return launched("nn_up2_concat_bwd");
+}
+
+int32_t nn_mse(const void* out, const float* target, const uint8_t* mask, const float* cw, void* dout, double* loss,
+               int64_t voxels, int32_t cpad, int32_t ct, double count, void* stream) {
+  if (!out || !target || !mask || !cw || !dout || !loss || voxels <= 0 || ct <= 0 || ct > cpad || !(count > 0))
+    return fail("nn_mse: bad arguments");
+  mse_kernel<<<blocks_for(voxels, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)out, target, mask, cw,
+                                                                         (bf16*)dout, loss, voxels, cpad, ct, count);
+  return launched("nn_mse");
+}
+
+int32_t nn_adam(float* w, const float* g, float* m, float* v, void* wb, int64_t count, float lr, float beta1,
+                float beta2, float eps, int32_t t, void* stream) {
+  if (!w || !g || !m || !v || count < 0 || t < 1) return fail("nn_adam: bad arguments");
+  if (count == 0) return 0;
+  const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
+  adam_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>(w, g, m, v, (bf16*)wb, count, lr, beta1, beta2,
+                                                                         eps, c1, c2);
+  return launched("nn_adam");
+}
+
+int32_t nn_diff_norms(const float* a, const float* b, int64_t count, double* out, void* stream) {
+  if (!a || !b || !out || count < 0) return fail("nn_diff_norms: bad arguments");
+  if (count == 0) return 0;
+  unsigned grid = blocks_for(count, 256 * 8);
+  if (grid > 2048) grid = 2048;
+  diff_norms_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(a, b, count, out);
+  return launched("nn_diff_norms");
+}
+
+int32_t nn_to_bf16(const float* x, void* y, int64_t count, void* stream) {
+  if (!x || !y || count < 0) return fail("nn_to_bf16: bad arguments");
+  if (count == 0) return 0;
+  to_bf16_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>(x, (bf16*)y, count);
+  return launched("nn_to_bf16");
+}
+
+int32_t nn_from_bf16(const void* x, float* y, int64_t count, void* stream) {
+  if (!x || !y || count < 0) return fail("nn_from_bf16: bad arguments");
+  if (count == 0) return 0;
+  from_bf16_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, y, count);
+  return launched("nn_from_bf16");
+}
+
+}  // extern "C"

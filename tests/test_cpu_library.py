@@ -41,6 +41,21 @@ def test_header_entry_points_are_exported():
     assert L.lbm_abi_version() == abi.ABI_VERSION
 
 
+def test_unet_header_entry_points_are_exported():
+    from lbm3d_bb_b200 import build, unet
+
+    if not unet.LIB_PATH.exists():
+        build.build_unet()
+    text = (ROOT / "include" / "unet3d.h").read_text()
+    declared = sorted(set(re.findall(r"^\s*(?:int32_t|const char\*)\s+(nn_\w+)\s*\(", text, re.M)))
+    nm = subprocess.run(["nm", "-D", "--defined-only", str(unet.LIB_PATH)], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\sT\s(nn_\w+)$", nm, re.M))
+    assert set(declared) <= exported, set(declared) - exported
+    assert set(declared) == set(unet.exported_symbols())
+    L = unet.lib()
+    assert L.nn_abi_version() == 1
+
+
 def test_lattice_constants():
     from lbm3d_bb_b200 import lattice
 
