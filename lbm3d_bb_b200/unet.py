@@ -273,11 +273,12 @@ class UNet3D:
         for g in self.G.values():
             g.zero_()
 
-    def loss_and_grad(self, target, mask, cw, count):
+    def loss_and_grad(self, target, mask, cw, count, accumulate=None):
         """Masked MSE of the last forward output; writes its gradient into the output
-        gradient buffer and returns the loss as a device FP64 scalar."""
+        gradient buffer and returns the loss as a device FP64 scalar (added into
+        `accumulate` when given)."""
         t = self.torch
-        loss = t.zeros(1, dtype=t.float64, device=self.dev)
+        loss = accumulate if accumulate is not None else t.zeros(1, dtype=t.float64, device=self.dev)
         geo = self.geo[1]
         vox = geo[0] * geo[1] * geo[2] * geo[3]
         self.ops.mse(self.A["out"], target, mask, cw, self.D["out"], loss, vox, count)

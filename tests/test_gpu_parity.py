@@ -63,6 +63,37 @@ def test_channel_outlets_fp64(gpu, oracle_lib, outlet, storage_steps):
     _force_close(g.force_history(1, storage_steps)[:, :3], o.force_history(1, storage_steps)[:, :3], TOL_FORCE)
 
 
+def test_rotated_ellipsoid_channel_fp64(gpu, oracle_lib):
+    """The warm-start workload's body: a rotated ellipsoid (flags and links bit-exact,
+    fields and forces after 30 steps)."""
+    import math
+
+    a, b = 0.7, -1.1
+    ca, sa, cb, sb = math.cos(a), math.sin(a), math.cos(b), math.sin(b)
+    rz = np.array([[ca, -sa, 0], [sa, ca, 0], [0, 0, 1]])
+    rx = np.array([[1, 0, 0], [0, cb, -sb], [0, sb, cb]])
+    rot = (rz @ rx).ravel()
+    faces = ("inlet", "pressure", "wall", "wall", "wall", "wall")
+
+    def make(cls):
+        d = cls(48, 24, 20, collision="BGK", storage="fp64", faces=faces, omega_p=1 / 0.7,
+                face_u=cases.face_u_inlet(0.05))
+        d.add_body(abi.make_body(abi.BODY_ELLIPSOID, (17.3, 11.8, 10.4), semi=(6.5, 3.2, 4.1), rot=rot))
+        d.init_equilibrium()
+        return d
+
+    g, o = make(Domain), make(OracleDomain)
+    for x, y in zip(g.flags(), o.flags()):
+        assert np.array_equal(x, y)
+    assert g.flags()[0].sum() > 200
+    for x, y in zip(g.links(), o.links()):
+        assert np.array_equal(x, y)
+    g.step(30)
+    o.step(30)
+    assert rel_l2(g.populations(), o.populations()) <= 1e-12
+    _force_close(g.force_history(1, 30)[:, :3], o.force_history(1, 30)[:, :3], TOL_FORCE)
+
+
 def test_sphere_channel_flags_links(gpu, oracle_lib):
     g = cases.sphere_channel(Domain)
     o = cases.sphere_channel(OracleDomain)
