@@ -291,7 +291,8 @@ typedef struct lbm_batch lbm_batch;
 int32_t lbm_batch_create(lbm_ctx* const* ctxs, int32_t count, lbm_batch** out);
 int32_t lbm_batch_destroy(lbm_batch* b);
 const char* lbm_batch_last_error(const lbm_batch* b);
-/* `nsteps` batched steps, enqueued as 2 launches per step. */
+/* `nsteps` batched steps, enqueued as 3 launches per step (the even-phase and the
+ * odd-phase kernel, each skipping the domains of the other phase, and the counter). */
 int32_t lbm_batch_step(lbm_batch* b, int32_t nsteps);
 /* Records `nsteps` batched steps into a CUDA graph (replacing an earlier one); runs
  * nothing.  The capture uses a private stream. */

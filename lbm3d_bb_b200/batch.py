@@ -30,7 +30,8 @@ class Batch:
             raise LbmError(st, (self._L.lbm_batch_last_error(self._h) or b"").decode(errors="replace"))
 
     def step(self, nsteps: int = 1) -> None:
-        """nsteps batched steps (two launches each: the step and the counter advance)."""
+        """nsteps batched steps (three launches each: the two phase kernels and the
+        counter advance)."""
         self._check(self._L.lbm_batch_step(self._h, int(nsteps)))
 
     def capture(self, nsteps: int) -> None:

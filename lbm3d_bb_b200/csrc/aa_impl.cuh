@@ -38,31 +38,43 @@
 namespace lbm {
 
 // ---- storage policies ------------------------------------------------------------
+// ld/st convert between the stored value and the population f; ld_raw/st_raw move
+// the stored value as it is.  DEV: the stored value is the deviation g = f - w_d rho0,
+// and the fast path computes in deviations (no conversion per population).
 struct StF32 {
   using S = float;
   using C = float;
   static constexpr int MIN_BLOCKS = LBM_MINB_F32;  // 256 x 4 threads -> at most 64 registers
+  static constexpr bool DEV = false;
   static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
   static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
+  static __device__ __forceinline__ C ld_raw(const S* p) { return *p; }
+  static __device__ __forceinline__ void st_raw(S* p, C v) { *p = v; }
 };
 struct StF64 {
   using S = double;
   using C = double;
   static constexpr int MIN_BLOCKS = 2;
+  static constexpr bool DEV = false;
   static __device__ __forceinline__ C ld(const S* p, int, C) { return *p; }
   static __device__ __forceinline__ void st(S* p, C v, int, C) { *p = v; }
+  static __device__ __forceinline__ C ld_raw(const S* p) { return *p; }
+  static __device__ __forceinline__ void st_raw(S* p, C v) { *p = v; }
 };
 // FP16 deviation from the rest equilibrium: stored h = f - w_d*rho0, computed in FP32.
 struct StF16 {
   using S = __half;
   using C = float;
   static constexpr int MIN_BLOCKS = LBM_MINB_F32;
+  static constexpr bool DEV = true;
   static __device__ __forceinline__ C ld(const S* p, int d, C rho0) {
     return wgt<float>(d) * rho0 + __half2float(*p);
   }
   static __device__ __forceinline__ void st(S* p, C v, int d, C rho0) {
     *p = __float2half_rn(v - wgt<float>(d) * rho0);
   }
+  static __device__ __forceinline__ C ld_raw(const S* p) { return __half2float(*p); }
+  static __device__ __forceinline__ void st_raw(S* p, C v) { *p = __float2half_rn(v); }
 };
 
 // ---- collision ---------------------------------------------------------------------
@@ -84,8 +96,11 @@ __device__ __forceinline__ double recip(double r) { return 1.0 / r; }
 // Moments from the nine opposite-direction pairs (d, d+1): s = f_d + f_{d+1},
 // t = f_d - f_{d+1}; rho = sum s + f_18, j = sum over pairs of c_d t.  Then
 // u = j/rho + g/2 (Guo).
-template <class C, bool FORCE>
-__device__ __forceinline__ void moments(const C* f, const Coll<C>& k, C& rho, C& ux, C& uy, C& uz) {
+// DEV: f holds deviations g = f - w rho0 (sum w = 1, sum w c = 0: rho = rho0 + sum g,
+// j = sum c g).
+template <class C, bool FORCE, bool DEV = false>
+__device__ __forceinline__ void moments(const C* f, const Coll<C>& k, C& rho, C& ux, C& uy, C& uz,
+                                        const C rho0 = C(0)) {
   C sp[9], tp[9];
 #pragma unroll
   for (int q = 0; q < 9; q++) {
@@ -104,6 +119,7 @@ __device__ __forceinline__ void moments(const C* f, const Coll<C>& k, C& rho, C&
     if (cz(d) == 1) jz += tp[q];
     if (cz(d) == -1) jz -= tp[q];
   }
+  if (DEV) r += rho0;
   const C inv = recip(r);
   rho = r;
   ux = jx * inv;
@@ -140,8 +156,12 @@ __device__ __forceinline__ C feq(int d, C rho, C ux, C uy, C uz) {
 // e = w rho (1 - 1.5 u^2 + 4.5 (c.u)^2) and an odd part o = 3 w rho (c.u), the Guo
 // source S_d = w [3 (c_d - u).F + 9 (c_d.u)(c_d.F)] into w (9 (c.u)(c.F) - 3 u.F) and
 // 3 w (c.F).  Relaxation rates and weights are folded per weight class.
-template <class C, bool TRT, bool FORCE>
-__device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rho, C ux, C uy, C uz) {
+// DEV: f and p are deviations g = f - w rho0.  Only the even equilibrium part carries
+// the offset: e - w rho0 = w (rho (1 - 1.5 u^2 + 4.5 (c.u)^2) - rho0); in the TRT form the
+// offsets of f+ and of e cancel because hp = om_p / 2.
+template <class C, bool TRT, bool FORCE, bool DEV = false>
+__device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rho, C ux, C uy, C uz,
+                                        const C rho0 = C(0)) {
   const C usq = ux * ux + uy * uy + uz * uz;
   const C base = C(1) - C(1.5) * usq;
   C Fx = C(0), Fy = C(0), Fz = C(0), m3uF = C(0);
@@ -155,7 +175,8 @@ __device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rh
   if (!TRT) {
     const C om = k.om_p, omc = C(1) - k.om_p;
     // omega * e = B + T (c.u)^2 ; omega * o = O (c.u)
-    const C B1 = om * wr1 * base, B2 = om * wr2 * base;
+    const C rb = rho * base - rho0;  // DEV only
+    const C B1 = DEV ? om * wgt<C>(0) * rb : om * wr1 * base, B2 = DEV ? om * wgt<C>(6) * rb : om * wr2 * base;
     const C T1 = C(4.5) * om * wr1, T2 = C(4.5) * om * wr2;
     const C O1 = C(3) * om * wr1, O2 = C(3) * om * wr2;
     const C fac = C(1) - C(0.5) * om;
@@ -176,7 +197,7 @@ __device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rh
       p[d] = omc * f[d] + (e + o);
       p[d + 1] = omc * f[d + 1] + (e - o);
     }
-    C e0 = om * wr0 * base;
+    C e0 = DEV ? om * wgt<C>(18) * rb : om * wr0 * base;
     if (FORCE) e0 += fac * wgt<C>(18) * m3uF;
     p[18] = omc * f[18] + e0;
   } else {
@@ -187,7 +208,7 @@ __device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rh
       const int d = 2 * q;
       const C wr = d < 6 ? wr1 : wr2;
       const C cu = cdot<C>(d, ux, uy, uz);
-      C e = wr * (base + C(4.5) * (cu * cu));
+      C e = DEV ? wgt<C>(d) * (rho * (base + C(4.5) * (cu * cu)) - rho0) : wr * (base + C(4.5) * (cu * cu));
       C o = (C(3) * wr) * cu;
       // A = om_p (f+ - e), Bm = om_m (f- - o), f+- = (f_d +- f_d+1)/2
       C A = hp * (f[d] + f[d + 1]) - k.om_p * e;
@@ -201,7 +222,7 @@ __device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rh
       p[d] = (f[d] - A) - Bm;
       p[d + 1] = (f[d + 1] - A) + Bm;
     }
-    C v = f[18] - k.om_p * (f[18] - wr0 * base);
+    C v = f[18] - k.om_p * (f[18] - (DEV ? wgt<C>(18) * (rho * base - rho0) : wr0 * base));
     if (FORCE) v += fac_p * wgt<C>(18) * m3uF;
     p[18] = v;
   }
@@ -269,10 +290,11 @@ __device__ __forceinline__ FaceLane face_lane(const Grid& g, int x, int y, int z
 // Boundary value of incoming direction d whose source lies outside a non-periodic
 // face (kept in the node's own slot A[d][x]).  At edges and corners the face of the
 // x axis wins, then y, then z.  xlo/xhi/ylo/yhi: the node lies on that face.
+// off: w_d rho0 when pst and the result are deviations (FP16 fast path), else 0.
 template <class C>
 __device__ __forceinline__ C face_value(const AAParams& p, const int d, const bool xlo, const bool xhi,
                                         const bool ylo, const bool yhi, const C rho, const C ux, const C uy,
-                                        const C uz, const C* pst) {
+                                        const C uz, const C* pst, const C off = C(0)) {
   const int o = opp(d);
   const bool xo = (cx(d) > 0 && xlo) || (cx(d) < 0 && xhi);
   const bool yo = (cy(d) > 0 && ylo) || (cy(d) < 0 && yhi);
@@ -282,12 +304,12 @@ __device__ __forceinline__ C face_value(const AAParams& p, const int d, const bo
   const C ufx = C(xo ? p.face_u[fx][0] : (yo ? p.face_u[fy][0] : p.face_u[fz][0]));
   const C ufy = C(xo ? p.face_u[fx][1] : (yo ? p.face_u[fy][1] : p.face_u[fz][1]));
   const C ufz = C(xo ? p.face_u[fx][2] : (yo ? p.face_u[fy][2] : p.face_u[fz][2]));
-  if (kind == LBM_FACE_EQ_INLET) return feq<C>(d, rho, ufx, ufy, ufz);
+  if (kind == LBM_FACE_EQ_INLET) return feq<C>(d, rho, ufx, ufy, ufz) - off;
   if (kind == LBM_FACE_OUTFLOW) return pst[d];
   if (kind == LBM_FACE_PRESSURE) {
     const C cu = cdot<C>(d, ux, uy, uz);
     const C usq = ux * ux + uy * uy + uz * uz;
-    return -pst[o] + C(2) * wgt<C>(d) * C(p.rho0) * (C(1) + C(4.5) * cu * cu - C(1.5) * usq);
+    return -pst[o] + C(2) * wgt<C>(d) * C(p.rho0) * (C(1) + C(4.5) * cu * cu - C(1.5) * usq) - C(2) * off;
   }
   return pst[o] - C(6) * wgt<C>(o) * rho * cdot<C>(o, ufx, ufy, ufz);
 }
@@ -449,6 +471,21 @@ __device__ __noinline__ void aa_general(const AAParams& p, typename SP::S* __res
 // The loads are split from the compute so that the caller can issue them before the
 // node's flag byte arrives (speculatively, for every lane whose coordinates allow
 // the fast path), instead of chaining two memory round trips.
+// Fast-path population access: the stored value itself when the storage keeps
+// deviations (computed in deviation form), the population otherwise.
+template <class SP>
+__device__ __forceinline__ typename SP::C ld_fast(const typename SP::S* p, int d, typename SP::C rho0) {
+  if (SP::DEV) return SP::ld_raw(p);
+  return SP::ld(p, d, rho0);
+}
+template <class SP>
+__device__ __forceinline__ void st_fast(typename SP::S* p, typename SP::C v, int d, typename SP::C rho0) {
+  if (SP::DEV)
+    SP::st_raw(p, v);
+  else
+    SP::st(p, v, d, rho0);
+}
+
 template <bool FACES>
 __device__ __forceinline__ void x_wrap_fix(const Grid& g, const int x, long long& fix_lo, long long& fix_hi) {
   const bool per = FACES ? g.per[0] != 0 : true;  // without FACES every axis is periodic
@@ -472,7 +509,7 @@ __device__ __forceinline__ void aa_fast_load(const AAParams& p, const typename S
       // source outside a face: the boundary value sits in the own slot
       if (FACES && d < 18 && ((face >> d) & 1u)) o = (long long)d * p.g.plane;
     }
-    f[d] = SP::ld(base + o, d, rho0);
+    f[d] = ld_fast<SP>(base + o, d, rho0);
   }
 }
 
@@ -487,14 +524,14 @@ __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S
   if (ODD && bc) {  // bounce-back values are kept in the own slots
 #pragma unroll
     for (int d = 0; d < 18; d++)
-      if ((bc >> d) & 1u) f[d] = SP::ld(base + (long long)d * p.g.plane, d, rho0);
+      if ((bc >> d) & 1u) f[d] = ld_fast<SP>(base + (long long)d * p.g.plane, d, rho0);
   }
   long long fix_lo = 0, fix_hi = 0;
   if (ODD) x_wrap_fix<FACES>(p.g, x, fix_lo, fix_hi);
   C rho, ux, uy, uz;
-  moments<C, FORCE>(f, k, rho, ux, uy, uz);
+  moments<C, FORCE, SP::DEV>(f, k, rho, ux, uy, uz, rho0);
   C pst[Q];
-  collide<C, TRT, FORCE>(f, pst, k, rho, ux, uy, uz);
+  collide<C, TRT, FORCE, SP::DEV>(f, pst, k, rho, ux, uy, uz, rho0);
   const uint32_t face = FACES ? fc.mask : 0u;
   // warps without a face node take the plain store loop; a warp with one runs the
   // per-direction face test on every lane (one loop, no divergence between loops)
@@ -511,13 +548,14 @@ __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S
         // the incoming direction whose source lies outside: j (even), opp(j) (odd)
         const int fd = ODD ? opp(j) : j;
         if ((face >> fd) & 1u) {
-          v = face_value<C>(p, fd, fc.xlo, fc.xhi, fc.ylo, fc.yhi, rho, ux, uy, uz, pst);
+          v = face_value<C>(p, fd, fc.xlo, fc.xhi, fc.ylo, fc.yhi, rho, ux, uy, uz, pst,
+                            SP::DEV ? wgt<C>(fd) * rho0 : C(0));
           if (ODD) o = (long long)fd * p.g.plane;
         } else if (ODD && ((bc >> fd) & 1u)) {
           o = (long long)fd * p.g.plane;
         }
       }
-      SP::st(base + o, v, j, rho0);
+      st_fast<SP>(base + o, v, j, rho0);
     }
   } else {
 #pragma unroll
@@ -528,7 +566,7 @@ __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S
         if (cx(j) == -1) o += fix_lo;
         if (j < 18 && ((bc >> opp(j)) & 1u)) o = (long long)opp(j) * p.g.plane;
       }
-      SP::st(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
+      st_fast<SP>(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
     }
   }
   if (bc && p.compute_force) {
@@ -537,7 +575,7 @@ __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S
     for (int d = 0; d < 18; d++) {
       if (!((bc >> d) & 1u)) continue;
       const int o = opp(d);
-      const double t = 2.0 * (double)pst[o];
+      const double t = 2.0 * (double)(SP::DEV ? pst[o] + wgt<C>(o) * rho0 : pst[o]);
       const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
       const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
       const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
@@ -647,7 +685,10 @@ __device__ __forceinline__ void divmod_rcp(const unsigned n, const int d, const 
 // and the force record of a domain follow from the device step counter, which a
 // one-thread kernel advances after every step: the same launch sequence can be
 // captured once in a CUDA graph and replayed.
-template <class SP, bool TRT, bool FORCE, bool FACES>
+// One kernel per phase: the ODD instance updates the domains whose phase this step is
+// odd and skips the others (both are launched every step), so each holds one phase's
+// code.
+template <class SP, bool ODD, bool TRT, bool FORCE, bool FACES>
 __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kernel(const __grid_constant__ BatchParams bp) {
   __shared__ AAParams sp;
   using S = typename SP::S;
@@ -655,7 +696,7 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
   const long long k = *bp.counter;
   const long long G = gridDim.x;
   const long long first = bp.items * blockIdx.x / G, last = bp.items * (blockIdx.x + 1) / G;
-  int dom = -1, phase = 0;
+  int dom = -1;
   S* A = nullptr;
   const uint8_t* flags = nullptr;
   double* rec = nullptr;
@@ -668,6 +709,11 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
   for (long long item = first; item < last; item++) {
     const int d = bp.item_dom[item];
     if (d != dom) {
+      const BatchDom& D = bp.doms[d];
+      if ((int)((D.phase0 + k) & 1) != (ODD ? 1 : 0)) {  // the other phase's kernel takes it
+        item = D.item_end - 1;
+        continue;
+      }
       if (dom >= 0 && sp.compute_force) {
         block_force_reduce(acc, has_link, rec + stripe);
 #pragma unroll
@@ -676,9 +722,7 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
       }
       __syncthreads();  // every thread is done with the previous parameter block
       dom = d;
-      const BatchDom& D = bp.doms[d];
-      phase = (int)((D.phase0 + k) & 1);
-      const int* src = reinterpret_cast<const int*>(&D.p[phase]);
+      const int* src = reinterpret_cast<const int*>(&D.p[ODD ? 1 : 0]);
       int* dst = reinterpret_cast<int*>(&sp);
       for (int w = t; w < (int)(sizeof(AAParams) / sizeof(int)); w += BATCH_ITEM) dst[w] = src[w];
       A = (S*)D.A;
@@ -702,10 +746,7 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
     int x, y;
     divmod_rcp(cell, g.nx, inv_nx, row, x);
     divmod_rcp(row, g.ny, inv_ny, z, y);
-    if (phase)
-      aa_direct<SP, true, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
-    else
-      aa_direct<SP, false, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
+    aa_direct<SP, ODD, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
   }
   if (dom >= 0 && sp.compute_force) block_force_reduce(acc, has_link, rec + stripe);
 }
@@ -846,7 +887,7 @@ __global__ void __launch_bounds__(128) aa_tma_kernel(const __grid_constant__ AAP
     for (int d = 0; d < Q; d++) {
       int idx = t;
       if (ODD) idx = cx(d) == 1 ? T.halo - 1 + t : (cx(d) == -1 ? t + 1 : t);
-      f[d] = SP::ld(st + d * T.buf_elems + idx, d, rho0);
+      f[d] = ld_fast<SP>(st + d * T.buf_elems + idx, d, rho0);
     }
     if (t == 0) pending &= ~(1u << s);
     if (!__syncthreads_and(ok)) {  // stage consumed (or a wait gave up everywhere)
@@ -854,9 +895,9 @@ __global__ void __launch_bounds__(128) aa_tma_kernel(const __grid_constant__ AAP
       break;
     }
     C rho, ux, uy, uz;
-    moments<C, FORCE>(f, kc, rho, ux, uy, uz);
+    moments<C, FORCE, SP::DEV>(f, kc, rho, ux, uy, uz, rho0);
     C pst[Q];
-    collide<C, TRT, FORCE>(f, pst, kc, rho, ux, uy, uz);
+    collide<C, TRT, FORCE, SP::DEV>(f, pst, kc, rho, ux, uy, uz, rho0);
     const long long i = row * g.nx + x;
     S* const base = A + i;
     long long fix_lo = 0, fix_hi = 0;
@@ -871,7 +912,7 @@ __global__ void __launch_bounds__(128) aa_tma_kernel(const __grid_constant__ AAP
         if (cx(j) == 1) o -= fix_hi;
         if (cx(j) == -1) o += fix_lo;
       }
-      SP::st(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
+      st_fast<SP>(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
     }
   }
   if (failed) {
@@ -1053,9 +1094,19 @@ static cudaError_t launch_sp(const AAParams& p, void* A, const uint8_t* flags, b
 // reports how many blocks of the kernel fit on one SM.
 template <class SP, bool TRT, bool FORCE, bool FACES>
 static cudaError_t batch_one(const BatchParams& bp, int blocks, int* per_sm, cudaStream_t s) {
-  auto kern = aa_batch_kernel<SP, TRT, FORCE, FACES>;
-  if (per_sm) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, BATCH_ITEM, 0);
-  kern<<<(unsigned)blocks, BATCH_ITEM, 0, s>>>(bp);
+  auto even = aa_batch_kernel<SP, false, TRT, FORCE, FACES>;
+  auto odd = aa_batch_kernel<SP, true, TRT, FORCE, FACES>;
+  if (per_sm) {
+    int a = 0, b = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, even, BATCH_ITEM, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, odd, BATCH_ITEM, 0);
+    *per_sm = a < b ? a : b;
+    return e;
+  }
+  even<<<(unsigned)blocks, BATCH_ITEM, 0, s>>>(bp);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  odd<<<(unsigned)blocks, BATCH_ITEM, 0, s>>>(bp);
   return cudaGetLastError();
 }
 

@@ -1204,7 +1204,7 @@ namespace {
 // ctx->nstep steps and its populations are in the `swapped` layout.
 void batch_entry(const lbm_batch* b, int m, BatchDom& e) {
   const lbm_ctx* c = b->ctxs[m];
-  const long long item_begin = e.item_begin;
+  const long long item_begin = e.item_begin, item_end = e.item_end;
   e = BatchDom{};
   fill_aa_params(c, e.p[0], false);
   fill_aa_params(c, e.p[1], true);
@@ -1215,6 +1215,7 @@ void batch_entry(const lbm_batch* b, int m, BatchDom& e) {
   e.base_step = c->nstep - b->k_host;
   e.phase0 = (int)(((c->swapped ? 1 : 0) - (b->k_host & 1) + 2) & 1);
   e.item_begin = item_begin;
+  e.item_end = item_end;
 }
 
 // Brings the device table in line with the members (a member stepped alone since the
@@ -1322,6 +1323,7 @@ int32_t lbm_batch_create(lbm_ctx* const* ctxs, int32_t count, lbm_batch** out) {
   for (int32_t m = 0; m < count; m++) {
     const long long n = (ctxs[m]->g.N + BATCH_ITEM - 1) / BATCH_ITEM;
     b->host[m].item_begin = next;
+    b->host[m].item_end = next + n;
     for (long long i = 0; i < n; i++) item_dom[(size_t)(next + i)] = m;
     next += n;
     batch_entry(b, m, b->host[m]);
@@ -1368,7 +1370,7 @@ int32_t lbm_batch_step(lbm_batch* b, int32_t nsteps) {
   if (rc) return rc;
   rc = batch_enqueue(b, nsteps, b->stream);
   if (rc) return rc;
-  b->launches += 2LL * nsteps;
+  b->launches += (long long)BATCH_LAUNCHES_PER_STEP * nsteps;
   for (lbm_ctx* c : b->ctxs) c->launches += nsteps;
   batch_advance_members(b, nsteps);
   return LBM_OK;
@@ -1415,7 +1417,7 @@ int32_t lbm_batch_replay(lbm_batch* b, int32_t times) {
   for (int32_t r = 0; r < times; r++)
     if (b->cuda(cudaGraphLaunch(b->exec, b->stream), "cudaGraphLaunch")) return LBM_ERR_CUDA;
   const long long n = (long long)times * b->graph_steps;
-  b->launches += 2 * n;
+  b->launches += (long long)BATCH_LAUNCHES_PER_STEP * n;
   for (lbm_ctx* c : b->ctxs) c->launches += n;
   batch_advance_members(b, n);
   return LBM_OK;

@@ -42,6 +42,7 @@ struct AAParams {
 
 // Batched step over many independent config-mode domains (one launch per step).
 constexpr int BATCH_ITEM = 128;  // cells per work item = threads per block
+constexpr int BATCH_LAUNCHES_PER_STEP = 3;  // even-phase and odd-phase kernels, counter advance
 
 struct BatchDom {
   AAParams p[2];         // parameter blocks of the even [0] and odd [1] phase
@@ -52,6 +53,7 @@ struct BatchDom {
   int phase0;            // phase of batch step 0 (0 even, 1 odd)
   long long base_step;   // steps the domain had completed before batch step 0
   long long item_begin;  // first work item of the domain
+  long long item_end;    // one past its last work item
 };
 
 struct BatchParams {

@@ -44,6 +44,8 @@ class Domain:
         self.shape = (int(nx), int(ny), int(nz))
         self.N = int(nx) * int(ny) * int(nz)
         self.mode = mode
+        self.device = int(device)
+        self.stream = None
         handle = C.c_void_p()
         check(self._L.lbm_create(C.byref(self.cfg), int(device), C.byref(handle)))
         self._h = handle
@@ -79,6 +81,7 @@ class Domain:
         """stream: a torch.cuda.Stream, a raw cudaStream_t int, or None."""
         h = getattr(stream, "cuda_stream", stream)
         self._check(self._L.lbm_set_stream(self._h, C.c_void_p(h or 0)))
+        self.stream = stream if hasattr(stream, "cuda_stream") else None
 
     def synchronize(self) -> None:
         self._check(self._L.lbm_synchronize(self._h))

@@ -131,7 +131,7 @@ def gpu_runner(storage: str = "fp32", chunk: int = 100, compare_steps: int = 50,
         for d in doms:
             d.close()
         return {"results": results, "cells": n_cells, "ms_per_step_batched_graph": ms_graph,
-                "ms_per_step_one_launch_per_domain": ms_single, "launches_per_step_batched": 2,
+                "ms_per_step_one_launch_per_domain": ms_single, "launches_per_step_batched": 3,
                 "launches_per_step_single": len(doms)}
 
     return run
