@@ -67,6 +67,12 @@ int32_t nn_adam(float* w, const float* g, float* m, float* v, void* wb, int64_t 
 /* out[0] += sum (a - b)^2 and out[1] += sum a^2 over `count` FP32 values (FP64 sums):
  * the relative change of a field between two checks of a run to steady state. */
 int32_t nn_diff_norms(const float* a, const float* b, int64_t count, double* out, void* stream);
+/* Network input of one channel case with an ellipsoid body (centre, row-major
+ * body->world rotation, semi-axes; lattice units), BF16 (nz, ny, nx, 16): solid mask
+ * (the solver's rasterisation), signed distance / 16 clipped to [-1, 4], re_feature,
+ * node position x/nx, y/ny, z/nz, zeros. */
+int32_t nn_features_ellipsoid(void* out, int32_t nx, int32_t ny, int32_t nz, const double* center,
+                              const double* rot, const double* semi, float re_feature, void* stream);
 /* FP32 -> BF16 (round to nearest even) and BF16 -> FP32. */
 int32_t nn_to_bf16(const float* x, void* y, int64_t count, void* stream);
 int32_t nn_from_bf16(const void* x, float* y, int64_t count, void* stream);

@@ -409,6 +409,54 @@ __global__ void diff_norms_kernel(const float* __restrict__ a, const float* __re
   }
 }
 
+struct Ellipsoid {
+  double center[3];
+  double rot[9];  // row-major body -> world
+  double semi[3];
+};
+
+// Inputs of one case: mask, approximate signed distance / 16 in [-1, 4], Re feature,
+// node position; the mask uses the solver's rasteriser expression with unfused
+// FP64 operations, so it matches the solver's solid flags.
+__global__ void features_kernel(bf16* __restrict__ out, int nx, int ny, int nz, Ellipsoid e, float re_feature) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)nx * ny * nz;
+  if (v >= n) return;
+  const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)(v / ((long long)nx * ny));
+  const double dx = __dadd_rn(x + 0.5, -e.center[0]);
+  const double dy = __dadd_rn(y + 0.5, -e.center[1]);
+  const double dz = __dadd_rn(z + 0.5, -e.center[2]);
+  const double* r = e.rot;
+  double b[3], q[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    b[k] = __dadd_rn(__dadd_rn(__dmul_rn(r[k], dx), __dmul_rn(r[3 + k], dy)), __dmul_rn(r[6 + k], dz));
+    q[k] = __ddiv_rn(b[k], e.semi[k]);
+  }
+  const double e2 = __dadd_rn(__dadd_rn(__dmul_rn(q[0], q[0]), __dmul_rn(q[1], q[1])), __dmul_rn(q[2], q[2]));
+  const double er = sqrt(e2);
+  double g2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const double t = b[k] / (e.semi[k] * e.semi[k]);
+    g2 += t * t;
+  }
+  const double grad = sqrt(g2) / fmax(er, 1e-12);
+  const double sdf = (er - 1.0) / fmax(grad, 1e-12);
+  float f[16];
+#pragma unroll
+  for (int c = 0; c < 16; c++) f[c] = 0.f;
+  f[0] = e2 <= 1.0 ? 1.f : 0.f;
+  f[1] = fminf(fmaxf((float)(sdf / 16.0), -1.f), 4.f);
+  f[2] = re_feature;
+  f[3] = (float)((x + 0.5) / nx);
+  f[4] = (float)((y + 0.5) / ny);
+  f[5] = (float)((z + 0.5) / nz);
+  uint32_t* o = reinterpret_cast<uint32_t*>(out + v * 16);
+#pragma unroll
+  for (int c = 0; c < 8; c++) o[c] = pack_bf16(f[2 * c], f[2 * c + 1]);
+}
+
 unsigned blocks_for(long long count, int per) { return (unsigned)((count + per - 1) / per); }
 
 bool geo_ok(int n, int d, int h, int w) { return n > 0 && d > 0 && h > 0 && w > 0; }
@@ -552,6 +600,20 @@ int32_t nn_diff_norms(const float* a, const float* b, int64_t count, double* out
   if (grid > 2048) grid = 2048;
   diff_norms_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(a, b, count, out);
   return launched("nn_diff_norms");
+}
+
+int32_t nn_features_ellipsoid(void* out, int32_t nx, int32_t ny, int32_t nz, const double* center,
+                              const double* rot, const double* semi, float re_feature, void* stream) {
+  if (!out || !center || !rot || !semi || nx <= 0 || ny <= 0 || nz <= 0) return fail("nn_features_ellipsoid: bad arguments");
+  Ellipsoid e{};
+  for (int k = 0; k < 3; k++) {
+    e.center[k] = center[k];
+    e.semi[k] = semi[k];
+  }
+  for (int k = 0; k < 9; k++) e.rot[k] = rot[k];
+  const long long n = (long long)nx * ny * nz;
+  features_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((bf16*)out, nx, ny, nz, e, re_feature);
+  return launched("nn_features_ellipsoid");
 }
 
 int32_t nn_to_bf16(const float* x, void* y, int64_t count, void* stream) {

@@ -55,6 +55,7 @@ def lib() -> C.CDLL:
         "nn_mse": (i32, [vp, vp, vp, vp, vp, vp, i64, i32, i32, f64, vp]),
         "nn_adam": (i32, [vp, vp, vp, vp, vp, i64, f32, f32, f32, f32, i32, vp]),
         "nn_diff_norms": (i32, [vp, vp, i64, vp, vp]),
+        "nn_features_ellipsoid": (i32, [vp, i32, i32, i32, vp, vp, vp, f32, vp]),
         "nn_to_bf16": (i32, [vp, vp, i64, vp]),
         "nn_from_bf16": (i32, [vp, vp, i64, vp]),
     }
@@ -69,7 +70,7 @@ def lib() -> C.CDLL:
 def exported_symbols() -> list[str]:
     return ["nn_abi_version", "nn_last_error", "nn_conv3d_fwd", "nn_conv3d_flip", "nn_conv3d_bwd_weight",
             "nn_bias_grad", "nn_relu_bwd", "nn_pool2", "nn_pool2_bwd", "nn_up2_concat", "nn_up2_concat_bwd",
-            "nn_mse", "nn_adam", "nn_diff_norms", "nn_to_bf16", "nn_from_bf16"]
+            "nn_mse", "nn_adam", "nn_diff_norms", "nn_features_ellipsoid", "nn_to_bf16", "nn_from_bf16"]
 
 
 def _ck(status: int) -> None:
@@ -127,6 +128,13 @@ class Ops:
     def diff_norms(self, a, b, out):
         _ck(self.L.nn_diff_norms(_p(a), _p(b), a.numel(), _p(out), self.s))
 
+    def features_ellipsoid(self, out, shape_xyz, center, rot, semi, re_feature):
+        c = (C.c_double * 3)(*center)
+        r = (C.c_double * 9)(*rot)
+        s = (C.c_double * 3)(*semi)
+        nx, ny, nz = shape_xyz
+        _ck(self.L.nn_features_ellipsoid(_p(out), nx, ny, nz, c, r, s, float(re_feature), self.s))
+
     def to_bf16(self, x, y):
         _ck(self.L.nn_to_bf16(_p(x), _p(y), x.numel(), self.s))
 
@@ -145,17 +153,17 @@ def layer_table(width: int = 16):
             ("head", w, OUT_CH, False)]
 
 
-def init_params(width: int = 16, seed: int = 0) -> dict[str, np.ndarray]:
+def init_params(width: int = 16, seed: int = 0, n_inputs: int = 6) -> dict[str, np.ndarray]:
     """He-normal weights [27][cout][cin] (the padded input/output channels zero), zero
     biases; FP32 numpy arrays keyed '<layer>.w' / '<layer>.b'."""
     rng = np.random.default_rng(seed)
     params = {}
     for name, cin, cout, relu in layer_table(width):
-        fan_in = 27 * (3 if name == "e1a" else cin)
+        fan_in = 27 * (n_inputs if name == "e1a" else cin)
         std = math.sqrt((2.0 if relu else 1.0) / fan_in)
         w = (rng.standard_normal((27, cout, cin)) * std).astype(np.float32)
         if name == "e1a":
-            w[:, :, 3:] = 0.0
+            w[:, :, n_inputs:] = 0.0
         if name == "head":
             w[:, N_TARGET:, :] = 0.0
         params[f"{name}.w"] = w

@@ -9,9 +9,11 @@ uniformly random orientation (unit quaternion from four normal deviates) and cen
 x in [24, 48], y and z in the central third; Re uniform in [10, 100] on the length
 L = 2 * (largest semi-axis), tau = 1/2 + 3 u L / Re.
 
-Network inputs (16 channels, 3 used): solid mask, approximate signed distance to the
-ellipsoid / 16 (clipped to [-1, 4]), (Re - 55) / 45.  Outputs: (rho - 1) / (3 u^2),
-u_x / u, u_y / u, u_z / u, trained with a masked MSE over the fluid nodes.
+Network inputs (16 channels, 6 used): solid mask, approximate signed distance to the
+ellipsoid / 16 (clipped to [-1, 4]), (Re - 55) / 45, and the node position x/NX, y/NY,
+z/NZ (without it the network cannot place the developing channel profile along x, which
+lies beyond its receptive field).  Outputs: (rho - 1) / (3 u^2), u_x / u, u_y / u,
+u_z / u, trained with a masked MSE over the fluid nodes (Adam, cosine learning-rate decay).
 
 A run is steady when the relative change of the field ||u(t) - u(t-100)|| / ||u(t)||
 falls below `tol` (data generation), and its drag is steady when the relative drag
@@ -19,7 +21,7 @@ change over 100 steps stays below `drag_tol` for three checks in a row (evaluati
 A warm start computes the first-step residual ||u(1) - u(0)|| / ||u(0)||; above
 `fallback` the case restarts from rest (the plain method remains the fallback).
 
-Usage (one GPU):  python -m lbm3d_bb_b200.warmstart --train 256 --heldout 32 --epochs 60 --out DIR
+Usage (one GPU):  python -m lbm3d_bb_b200.warmstart --train 256 --heldout 64 --epochs 200 --out DIR
 """
 from __future__ import annotations
 
@@ -70,9 +72,20 @@ def make_domain(p: dict, storage: str = "fp32", device: int = 0, stream=None, hi
     return d
 
 
+N_FEATURES = 6
+_GRID = None
+
+
+def _grid():
+    global _GRID
+    if _GRID is None:
+        _GRID = np.meshgrid(np.arange(NZ) + 0.5, np.arange(NY) + 0.5, np.arange(NX) + 0.5, indexing="ij")
+    return _GRID
+
+
 def features(p: dict) -> np.ndarray:
     """(NZ, NY, NX, 16) float32 network input of a case."""
-    z, y, x = np.meshgrid(np.arange(NZ) + 0.5, np.arange(NY) + 0.5, np.arange(NX) + 0.5, indexing="ij")
+    z, y, x = _grid()
     r = np.asarray(p["rot"]).reshape(3, 3)
     dx, dy, dz = x - p["center"][0], y - p["center"][1], z - p["center"][2]
     b = [(r[0, k] * dx + r[1, k] * dy) + r[2, k] * dz for k in range(3)]
@@ -86,7 +99,15 @@ def features(p: dict) -> np.ndarray:
     f[..., 0] = e2 <= 1.0
     f[..., 1] = np.clip(sdf / 16.0, -1.0, 4.0)
     f[..., 2] = (p["Re"] - 55.0) / 45.0
+    f[..., 3] = x / NX
+    f[..., 4] = y / NY
+    f[..., 5] = z / NZ
     return f
+
+
+def features_device(p: dict, out, ops) -> None:
+    """features(p) computed on the GPU into a BF16 (NZ, NY, NX, 16) tensor."""
+    ops.features_ellipsoid(out, (NX, NY, NZ), p["center"], p["rot"], p["semi"], (p["Re"] - 55.0) / 45.0)
 
 
 def target_of(rho, u, v, w) -> np.ndarray:
@@ -149,8 +170,7 @@ class Stepper:
         for k, d in enumerate(self.doms):
             n = d.step_count
             if n - self.check >= 1:
-                h = d.force_history(n - self.check, self.check + 1)
-                out[k] = (h[0, 0], h[-1, 0])
+                out[k] = (d.force(n - self.check)[0], d.force(n)[0])
         return out
 
     def close(self):
@@ -194,9 +214,8 @@ def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int 
                            "stable": ok})
             if not ok:
                 continue
-            x = torch.from_numpy(features(p)).to(dev)
-            xb = torch.empty(x.shape, dtype=torch.bfloat16, device=dev)
-            ops.to_bf16(x, xb)
+            xb = torch.empty((NZ, NY, NX, 16), dtype=torch.bfloat16, device=dev)
+            features_device(p, xb, ops)
             feats.append(xb)
             targs.append(torch.from_numpy(target_of(rho, u, v, w)).to(dev))
             m = (d.flags()[0] == 0).reshape(NZ, NY, NX).astype(np.uint8)
@@ -206,9 +225,11 @@ def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int 
     return torch.stack(feats), torch.stack(targs), torch.stack(masks), np.array(counts), record
 
 
-def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3, seed: int = 0, log=print):
+def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3, seed: int = 0, log=print,
+          lr_min: float = 1e-5):
     """Adam on the masked MSE over the GPU-resident data set (shuffled mini-batches
-    gathered by index).  Returns the per-epoch mean loss."""
+    gathered by index), learning rate decayed from lr to lr_min on a cosine.  Returns
+    the per-epoch mean loss."""
     import torch
 
     dev = model.dev
@@ -218,6 +239,8 @@ def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3,
     rng = np.random.default_rng(seed)
     hist = []
     nb = max(1, n // batch)
+    total = max(1, epochs * nb)
+    t = 0
     for ep in range(epochs):
         order = rng.permutation(n)
         acc.zero_()
@@ -229,7 +252,8 @@ def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3,
                                 accumulate=acc)
             model.zero_grad()
             model.backward(model.D["out"])
-            model.adam_step(lr=lr)
+            model.adam_step(lr=lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * t / total)))
+            t += 1
         hist.append(float(acc.item()) / nb)
         if ep % 10 == 0 or ep == epochs - 1:
             log(f"epoch {ep}: loss {hist[-1]:.5f}")
@@ -244,9 +268,9 @@ def predict(model, params: Sequence[dict], batch: int = 4):
     dev = model.dev
     for b0 in range(0, len(params), batch):
         ps = params[b0:b0 + batch]
-        x = torch.from_numpy(np.stack([features(p) for p in ps])).to(dev)
-        xb = torch.empty(x.shape, dtype=torch.bfloat16, device=dev)
-        model.ops.to_bf16(x, xb)
+        xb = torch.empty((len(ps), NZ, NY, NX, 16), dtype=torch.bfloat16, device=dev)
+        for k, p in enumerate(ps):
+            features_device(p, xb[k], model.ops)
         y = model.forward(xb)
         yf = torch.empty(y.shape, dtype=torch.float32, device=dev)
         model.ops.from_bf16(y, yf)
@@ -304,10 +328,11 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=256)
     ap.add_argument("--heldout", type=int, default=32)
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--max-steps", type=int, default=30000)
+    ap.add_argument("--max-steps", type=int, default=40000, help="cap of the data-generation runs")
+    ap.add_argument("--eval-max-steps", type=int, default=60000, help="cap of the evaluation runs")
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--drag-tol", type=float, default=1e-5)
     ap.add_argument("--fallback", type=float, default=0.05)
@@ -355,9 +380,9 @@ def _run(args, stream, out, log):
     e1.record(stream)
     e1.synchronize()
     infer_ms = e0.elapsed_time(e1)
-    warm = run_to_steady_drag(params, 0, stream, init=init, drag_tol=args.drag_tol, max_steps=args.max_steps,
+    warm = run_to_steady_drag(params, 0, stream, init=init, drag_tol=args.drag_tol, max_steps=args.eval_max_steps,
                               fallback=args.fallback)
-    rest = run_to_steady_drag(params, 0, stream, init=None, drag_tol=args.drag_tol, max_steps=args.max_steps)
+    rest = run_to_steady_drag(params, 0, stream, init=None, drag_tol=args.drag_tol, max_steps=args.eval_max_steps)
     ok = (warm["steps"] > 0) & (rest["steps"] > 0)
     err = np.abs(warm["drag"] - rest["drag"]) / np.maximum(np.abs(rest["drag"]), 1e-30)
     res = {

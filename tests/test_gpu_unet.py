@@ -192,3 +192,23 @@ def test_training_reduces_loss(gpu):
     assert np.isfinite(losses).all()
     assert losses[-1] < 0.6 * losses[0], losses[::10]
     assert losses[-1] < min(losses[:10])
+
+
+def test_features_on_gpu_match_host(gpu):
+    import torch
+
+    from lbm3d_bb_b200 import warmstart as W
+
+    ops = N.Ops()
+    for seed in (0, 7, 100003):
+        p = W.case_params(seed)
+        f = W.features(p)
+        out = torch.empty((W.NZ, W.NY, W.NX, 16), dtype=torch.bfloat16, device="cuda")
+        W.features_device(p, out, ops)
+        g = _host(out, ops)
+        assert np.array_equal(g[..., 0], f[..., 0])  # the solver's mask, bit for bit
+        assert np.abs(g[..., 1:] - U.to_bf16(f[..., 1:])).max() <= 2 ** -7 * 4
+        # and the solver rasterises the same solid nodes
+        d = W.make_domain(p)
+        assert np.array_equal(d.flags()[0].reshape(W.NZ, W.NY, W.NX), f[..., 0].astype(np.uint8))
+        d.close()
