@@ -73,6 +73,12 @@ int32_t nn_diff_norms(const float* a, const float* b, int64_t count, double* out
  * node position x/nx, y/ny, z/nz, zeros. */
 int32_t nn_features_ellipsoid(void* out, int32_t nx, int32_t ny, int32_t nz, const double* center,
                               const double* rot, const double* semi, float re_feature, void* stream);
+/* out (n, 4, d, h, w), FP32 planar: = (or += when accumulate != 0) weight * the first
+ * four channels of the network output y (n, d, h, w, 16), read from its mirror image in
+ * y (flip_y) and/or z (flip_z) with the mirrored velocity components (channels 2, 3)
+ * negated — the prediction for a reflected input mapped back to the original frame. */
+int32_t nn_unpack_fields(const void* y, float* out, int32_t n, int32_t d, int32_t h, int32_t wd, int32_t flip_y,
+                         int32_t flip_z, float weight, int32_t accumulate, void* stream);
 /* FP32 -> BF16 (round to nearest even) and BF16 -> FP32. */
 int32_t nn_to_bf16(const float* x, void* y, int64_t count, void* stream);
 int32_t nn_from_bf16(const void* x, float* y, int64_t count, void* stream);

@@ -702,6 +702,12 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
   double* rec = nullptr;
   long long item0 = 0;
   double inv_nx = 0.0, inv_ny = 0.0;
+  // With a non-periodic x axis the cells are numbered interior columns first
+  // (x = 1 .. nx-2, row by row), then the two face columns (x = 0 and nx-1 of each
+  // row, alternating), so that inlet/outlet nodes fill warps of their own instead of
+  // putting a face lane into almost every warp.
+  int xlo = 0, xint = 1;
+  unsigned n_int = 0;
   // force / torque of the current domain, reduced once per domain and block
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool has_link = false;
@@ -735,7 +741,11 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
         for (int w = t; w < FORCE_RECORD; w += BATCH_ITEM) next[w] = 0.0;
       }
       __syncthreads();
-      inv_nx = 1.0 / (double)sp.g.nx;
+      const bool split = !sp.g.per[0] && sp.g.nx > 2;
+      xlo = split ? 1 : 0;
+      xint = split ? sp.g.nx - 2 : sp.g.nx;
+      n_int = (unsigned)xint * (unsigned)sp.g.ny * (unsigned)sp.g.nz;
+      inv_nx = 1.0 / (double)xint;
       inv_ny = 1.0 / (double)sp.g.ny;
     }
     const Grid& g = sp.g;
@@ -744,7 +754,14 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
     const bool inb = cell < (unsigned)g.N;
     unsigned row, z;
     int x, y;
-    divmod_rcp(cell, g.nx, inv_nx, row, x);
+    if (cell < n_int) {
+      divmod_rcp(cell, xint, inv_nx, row, x);
+      x += xlo;
+    } else {  // face columns: (row, side) pairs
+      const unsigned f = cell - n_int;
+      row = f >> 1;
+      x = (f & 1u) ? g.nx - 1 : 0;
+    }
     divmod_rcp(row, g.ny, inv_ny, z, y);
     aa_direct<SP, ODD, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
   }

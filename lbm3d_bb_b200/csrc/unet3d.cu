@@ -457,6 +457,33 @@ __global__ void features_kernel(bf16* __restrict__ out, int nx, int ny, int nz, 
   for (int c = 0; c < 8; c++) o[c] = pack_bf16(f[2 * c], f[2 * c + 1]);
 }
 
+// out (n, 4, d, h, w) FP32 (+)= weight * the first four channels of y (n, d, h, w, 16),
+// read from the mirror image in y and/or z, with the mirrored velocity components
+// (channel 2 = u_y, 3 = u_z) negated: undoes a reflection of the input.
+__global__ void unpack_fields_kernel(const bf16* __restrict__ y, float* __restrict__ out, Geo g, int flip_y, int flip_z,
+                                     float weight, int accumulate, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;  // count = n * d * h * w
+  long long t = i;
+  const int x = (int)(t % g.w);
+  t /= g.w;
+  const int yy = (int)(t % g.h);
+  t /= g.h;
+  const int z = (int)(t % g.d);
+  const int n = (int)(t / g.d);
+  const int ys = flip_y ? g.h - 1 - yy : yy, zs = flip_z ? g.d - 1 - z : z;
+  const long long src = (((long long)n * g.d + zs) * g.h + ys) * g.w + x;
+  const long long plane = (long long)g.d * g.h * g.w;
+  const long long v = ((long long)z * g.h + yy) * g.w + x;
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    float val = __bfloat162float(y[src * 16 + c]) * weight;
+    if ((c == 2 && flip_y) || (c == 3 && flip_z)) val = -val;
+    float* o = out + ((long long)n * 4 + c) * plane + v;
+    *o = accumulate ? *o + val : val;
+  }
+}
+
 unsigned blocks_for(long long count, int per) { return (unsigned)((count + per - 1) / per); }
 
 bool geo_ok(int n, int d, int h, int w) { return n > 0 && d > 0 && h > 0 && w > 0; }
@@ -614,6 +641,15 @@ int32_t nn_features_ellipsoid(void* out, int32_t nx, int32_t ny, int32_t nz, con
   const long long n = (long long)nx * ny * nz;
   features_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((bf16*)out, nx, ny, nz, e, re_feature);
   return launched("nn_features_ellipsoid");
+}
+
+int32_t nn_unpack_fields(const void* y, float* out, int32_t n, int32_t d, int32_t h, int32_t wd, int32_t flip_y,
+                         int32_t flip_z, float weight, int32_t accumulate, void* stream) {
+  if (!y || !out || !geo_ok(n, d, h, wd)) return fail("nn_unpack_fields: bad arguments");
+  const long long count = (long long)n * d * h * wd;
+  unpack_fields_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>(
+      (const bf16*)y, out, Geo{n, d, h, wd}, flip_y, flip_z, weight, accumulate, count);
+  return launched("nn_unpack_fields");
 }
 
 int32_t nn_to_bf16(const float* x, void* y, int64_t count, void* stream) {

@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
         "nn_adam": (i32, [vp, vp, vp, vp, vp, i64, f32, f32, f32, f32, i32, vp]),
         "nn_diff_norms": (i32, [vp, vp, i64, vp, vp]),
         "nn_features_ellipsoid": (i32, [vp, i32, i32, i32, vp, vp, vp, f32, vp]),
+        "nn_unpack_fields": (i32, [vp, vp, i32, i32, i32, i32, i32, i32, f32, i32, vp]),
         "nn_to_bf16": (i32, [vp, vp, i64, vp]),
         "nn_from_bf16": (i32, [vp, vp, i64, vp]),
     }
@@ -70,7 +71,8 @@ def lib() -> C.CDLL:
 def exported_symbols() -> list[str]:
     return ["nn_abi_version", "nn_last_error", "nn_conv3d_fwd", "nn_conv3d_flip", "nn_conv3d_bwd_weight",
             "nn_bias_grad", "nn_relu_bwd", "nn_pool2", "nn_pool2_bwd", "nn_up2_concat", "nn_up2_concat_bwd",
-            "nn_mse", "nn_adam", "nn_diff_norms", "nn_features_ellipsoid", "nn_to_bf16", "nn_from_bf16"]
+            "nn_mse", "nn_adam", "nn_diff_norms", "nn_features_ellipsoid", "nn_unpack_fields", "nn_to_bf16",
+            "nn_from_bf16"]
 
 
 def _ck(status: int) -> None:
@@ -134,6 +136,11 @@ class Ops:
         s = (C.c_double * 3)(*semi)
         nx, ny, nz = shape_xyz
         _ck(self.L.nn_features_ellipsoid(_p(out), nx, ny, nz, c, r, s, float(re_feature), self.s))
+
+    def unpack_fields(self, y, out, shape, flip_y, flip_z, weight, accumulate):
+        n, d, h, wd = shape
+        _ck(self.L.nn_unpack_fields(_p(y), _p(out), n, d, h, wd, int(flip_y), int(flip_z), float(weight),
+                                    int(accumulate), self.s))
 
     def to_bf16(self, x, y):
         _ck(self.L.nn_to_bf16(_p(x), _p(y), x.numel(), self.s))

@@ -105,6 +105,38 @@ def features(p: dict) -> np.ndarray:
     return f
 
 
+REFLECTIONS = ((False, False), (True, False), (False, True), (True, True))  # (mirror y, mirror z)
+
+
+def reflect(p: dict, flip_y: bool, flip_z: bool) -> dict:
+    """The case mirrored about the channel's mid-plane(s): the ellipsoid's centre is
+    mirrored and its rotation becomes F R F (F = the mirror), a proper rotation of the
+    mirrored body; flow fields mirror with u_y (u_z) negated."""
+    f = np.diag([1.0, -1.0 if flip_y else 1.0, -1.0 if flip_z else 1.0])
+    r = np.asarray(p["rot"]).reshape(3, 3)
+    c = list(p["center"])
+    if flip_y:
+        c[1] = NY - c[1]
+    if flip_z:
+        c[2] = NZ - c[2]
+    q = dict(p)
+    q["center"] = c
+    q["rot"] = (f @ r @ f).ravel().tolist()
+    return q
+
+
+def mirror_target(t: np.ndarray, flip_y: bool, flip_z: bool) -> np.ndarray:
+    """Target (NZ, NY, NX, 4) of the mirrored case."""
+    t = t[:, ::-1] if flip_y else t
+    t = t[::-1] if flip_z else t
+    t = np.array(t)
+    if flip_y:
+        t[..., 2] = -t[..., 2]
+    if flip_z:
+        t[..., 3] = -t[..., 3]
+    return t
+
+
 def features_device(p: dict, out, ops) -> None:
     """features(p) computed on the GPU into a BF16 (NZ, NY, NX, 16) tensor."""
     ops.features_ellipsoid(out, (NX, NY, NZ), p["center"], p["rot"], p["semi"], (p["Re"] - 55.0) / 45.0)
@@ -180,10 +212,11 @@ class Stepper:
 
 
 def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int = 30000, tol: float = 1e-6,
-             group: int = 64, log=print):
+             group: int = 64, log=print, augment: bool = True):
     """Steady states of the cases, kept on the GPU: BF16 features (n, NZ, NY, NX, 16),
     FP32 targets (n, NZ, NY, NX, 4), fluid masks, fluid counts, and the record of
-    each run (steps, stability)."""
+    each run (steps, stability).  With `augment`, each steady state also enters in its
+    three mirror images (y, z, both)."""
     import torch
 
     from .unet import Ops
@@ -214,13 +247,17 @@ def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int 
                            "stable": ok})
             if not ok:
                 continue
-            xb = torch.empty((NZ, NY, NX, 16), dtype=torch.bfloat16, device=dev)
-            features_device(p, xb, ops)
-            feats.append(xb)
-            targs.append(torch.from_numpy(target_of(rho, u, v, w)).to(dev))
-            m = (d.flags()[0] == 0).reshape(NZ, NY, NX).astype(np.uint8)
-            masks.append(torch.from_numpy(m).to(dev))
-            counts.append(int(m.sum()))
+            t0_ = target_of(rho, u, v, w)
+            m0 = (d.flags()[0] == 0).reshape(NZ, NY, NX).astype(np.uint8)
+            for fy, fz in (REFLECTIONS if augment else REFLECTIONS[:1]):
+                xb = torch.empty((NZ, NY, NX, 16), dtype=torch.bfloat16, device=dev)
+                features_device(reflect(p, fy, fz), xb, ops)
+                feats.append(xb)
+                targs.append(torch.from_numpy(mirror_target(t0_, fy, fz)).to(dev))
+                m = m0[:, ::-1] if fy else m0
+                m = np.ascontiguousarray(m[::-1] if fz else m)
+                masks.append(torch.from_numpy(m).to(dev))
+                counts.append(int(m.sum()))
         st.close()
     return torch.stack(feats), torch.stack(targs), torch.stack(masks), np.array(counts), record
 
@@ -260,24 +297,25 @@ def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3,
     return hist
 
 
-def predict(model, params: Sequence[dict], batch: int = 4):
-    """Equilibrium initial fields (rho, u, v, w as FP64 host arrays) per case."""
+def predict(model, params: Sequence[dict], mirror_average: bool = True):
+    """Equilibrium initial fields (rho, u, v, w as FP64 host arrays) per case; with
+    `mirror_average` the network sees the case in its four mirror images (one batch)
+    and the predictions, mapped back, are averaged."""
     import torch
 
     out = []
     dev = model.dev
-    for b0 in range(0, len(params), batch):
-        ps = params[b0:b0 + batch]
-        xb = torch.empty((len(ps), NZ, NY, NX, 16), dtype=torch.bfloat16, device=dev)
-        for k, p in enumerate(ps):
-            features_device(p, xb[k], model.ops)
+    refl = REFLECTIONS if mirror_average else REFLECTIONS[:1]
+    xb = torch.empty((len(refl), NZ, NY, NX, 16), dtype=torch.bfloat16, device=dev)
+    acc = torch.empty((1, 4, NZ, NY, NX), dtype=torch.float32, device=dev)
+    for p in params:
+        for k, (fy, fz) in enumerate(refl):
+            features_device(reflect(p, fy, fz), xb[k], model.ops)
         y = model.forward(xb)
-        yf = torch.empty(y.shape, dtype=torch.float32, device=dev)
-        model.ops.from_bf16(y, yf)
-        yh = yf.cpu().numpy().astype(np.float64)
-        for k in range(len(ps)):
-            o = yh[k].reshape(-1, 16)
-            out.append((1.0 + RHO_SCALE * o[:, 0], U_IN * o[:, 1], U_IN * o[:, 2], U_IN * o[:, 3]))
+        for k, (fy, fz) in enumerate(refl):
+            model.ops.unpack_fields(y[k:k + 1], acc, (1, NZ, NY, NX), fy, fz, 1.0 / len(refl), k > 0)
+        o = acc.cpu().numpy().reshape(4, -1).astype(np.float64)
+        out.append((1.0 + RHO_SCALE * o[0], U_IN * o[1], U_IN * o[2], U_IN * o[3]))
     return out
 
 

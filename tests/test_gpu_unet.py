@@ -212,3 +212,25 @@ def test_features_on_gpu_match_host(gpu):
         d = W.make_domain(p)
         assert np.array_equal(d.flags()[0].reshape(W.NZ, W.NY, W.NX), f[..., 0].astype(np.uint8))
         d.close()
+
+
+@pytest.mark.parametrize("fy,fz", [(False, False), (True, False), (False, True), (True, True)])
+def test_unpack_fields_undoes_mirroring(ops, fy, fz):
+    import torch
+
+    rng = np.random.default_rng(2)
+    shape = (2, 4, 6, 16)
+    y = U.to_bf16(rng.standard_normal(shape + (16,)))
+    acc = torch.full((2, 4) + shape[1:], 7.0, dtype=torch.float32, device="cuda")
+    ops.unpack_fields(_dev(y, ops), acc, shape, fy, fz, 0.5, False)
+    ref = y[..., :4].copy()
+    if fy:
+        ref = ref[:, :, ::-1]
+        ref[..., 2] *= -1
+    if fz:
+        ref = ref[:, ::-1]
+        ref[..., 3] *= -1
+    ref = 0.5 * np.moveaxis(ref, -1, 1)
+    assert np.array_equal(_host(acc, ops), ref)
+    ops.unpack_fields(_dev(y, ops), acc, shape, fy, fz, 0.5, True)
+    assert np.array_equal(_host(acc, ops), 2 * ref)
