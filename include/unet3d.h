@@ -33,6 +33,14 @@ const char* nn_last_error(void);
 /* out = act(conv3x3x3(in, w) + bias); act = ReLU when relu != 0.  bias may be NULL. */
 int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* out, int32_t n, int32_t d,
                       int32_t h, int32_t wd, int32_t cin, int32_t cout, int32_t relu, void* stream);
+/* Engine of nn_conv3d_fwd (and so of the data gradient): 0 = mma.sync warp tiles
+ * (FP32 accumulation in registers), 1 = tcgen05 (128-voxel CTA tiles, operands in
+ * shared memory, FP32 accumulator in tensor memory).  Returns the previous engine, or
+ * nonzero with nn_last_error() for an unknown engine.  Process-wide. */
+int32_t nn_set_conv_engine(int32_t engine);
+/* Blocking: nonzero (and cleared) when a tcgen05 convolution gave up waiting for its
+ * matrix multiply since the last call; its output is then not valid. */
+int32_t nn_tc_status(void* stream);
 /* Weights of the data gradient: wt[26 - tap][ci][co] = w[tap][co][ci]; then
  * din = nn_conv3d_fwd(dout, wt, NULL, din, ..., cin = cout, cout = cin, relu = 0). */
 int32_t nn_conv3d_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream);

@@ -34,6 +34,9 @@
 #ifndef LBM_MINB_F32
 #define LBM_MINB_F32 4
 #endif
+#ifndef LBM_MINB_F16
+#define LBM_MINB_F16 4
+#endif
 
 namespace lbm {
 
@@ -65,7 +68,7 @@ struct StF64 {
 struct StF16 {
   using S = __half;
   using C = float;
-  static constexpr int MIN_BLOCKS = LBM_MINB_F32;
+  static constexpr int MIN_BLOCKS = LBM_MINB_F16;
   static constexpr bool DEV = true;
   static __device__ __forceinline__ C ld(const S* p, int d, C rho0) {
     return wgt<float>(d) * rho0 + __half2float(*p);
@@ -702,12 +705,6 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
   double* rec = nullptr;
   long long item0 = 0;
   double inv_nx = 0.0, inv_ny = 0.0;
-  // With a non-periodic x axis the cells are numbered interior columns first
-  // (x = 1 .. nx-2, row by row), then the two face columns (x = 0 and nx-1 of each
-  // row, alternating), so that inlet/outlet nodes fill warps of their own instead of
-  // putting a face lane into almost every warp.
-  int xlo = 0, xint = 1;
-  unsigned n_int = 0;
   // force / torque of the current domain, reduced once per domain and block
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool has_link = false;
@@ -741,27 +738,18 @@ __global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kerne
         for (int w = t; w < FORCE_RECORD; w += BATCH_ITEM) next[w] = 0.0;
       }
       __syncthreads();
-      const bool split = !sp.g.per[0] && sp.g.nx > 2;
-      xlo = split ? 1 : 0;
-      xint = split ? sp.g.nx - 2 : sp.g.nx;
-      n_int = (unsigned)xint * (unsigned)sp.g.ny * (unsigned)sp.g.nz;
-      inv_nx = 1.0 / (double)xint;
+      inv_nx = 1.0 / (double)sp.g.nx;
       inv_ny = 1.0 / (double)sp.g.ny;
     }
     const Grid& g = sp.g;
-    // a domain holds fewer than 2^31 cells: 32-bit index arithmetic
+    // a domain holds fewer than 2^31 cells: 32-bit index arithmetic.  Cells keep the
+    // row order (x fastest): ordering the x-face columns apart made their warps read
+    // 19 x 32 separate sectors (stride nx) and was slower overall.
     const unsigned cell = (unsigned)(item - item0) * BATCH_ITEM + t;
     const bool inb = cell < (unsigned)g.N;
     unsigned row, z;
     int x, y;
-    if (cell < n_int) {
-      divmod_rcp(cell, xint, inv_nx, row, x);
-      x += xlo;
-    } else {  // face columns: (row, side) pairs
-      const unsigned f = cell - n_int;
-      row = f >> 1;
-      x = (f & 1u) ? g.nx - 1 : 0;
-    }
+    divmod_rcp(cell, g.nx, inv_nx, row, x);
     divmod_rcp(row, g.ny, inv_ny, z, y);
     aa_direct<SP, ODD, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
   }

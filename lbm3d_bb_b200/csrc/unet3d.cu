@@ -145,6 +145,182 @@ __global__ void __launch_bounds__(128) conv_fwd_kernel(const bf16* __restrict__ 
   }
 }
 
+// ---- forward convolution on the 5th-generation tensor cores (tcgen05) ----------------
+// A CTA owns 128 consecutive voxels (M = 128) and all output channels (N = Cout); the
+// K loop runs over 27 taps x 16-channel slices, one tcgen05.mma (K = 16) each.  Every
+// thread gathers its voxel's 16 channels of the tap's neighbour into the A tile and the
+// CTA copies the tap's 16 x Cout weights into the B tile, both in the K-major
+// "interleaved" core-matrix layout (8 rows x 16 bytes per core matrix); two stages, so
+// the next gather overlaps the running MMA.  One thread issues the MMA and commits it
+// to the stage's mbarrier; the FP32 accumulator lives in tensor memory (TMEM) and is
+// read back with tcgen05.ld for the bias / ReLU / BF16 epilogue.  Every wait is
+// bounded: a wait that gives up sets the error word and the CTA still frees its TMEM.
+constexpr int TC_M = 128;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, K-major, no swizzle: start, leading-dimension byte
+// offset (between the two 8-element K halves), stride byte offset (between 8-row
+// groups), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 accumulator, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool tc_mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  for (int it = 0; it < (1 << 22); it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <int COUT>
+__global__ void __launch_bounds__(TC_M) conv_fwd_tc_kernel(const bf16* __restrict__ in, const bf16* __restrict__ w,
+                                                           const float* __restrict__ bias, bf16* __restrict__ out,
+                                                           const Geo g, const int cin, const int relu,
+                                                           const long long voxels, int* err) {
+  constexpr int NCOL = COUT <= 32 ? 32 : (COUT <= 64 ? 64 : 128);  // TMEM columns: a power of two >= 32
+  constexpr uint32_t A_LBO = TC_M * 16, B_LBO = COUT * 16;          // bytes per K half
+  __shared__ __align__(128) uint8_t sA[2][2 * A_LBO];
+  __shared__ __align__(128) uint8_t sB[2][2 * B_LBO];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
+                 "r"(NCOL)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    tc_mbar_init(&bar[0]);
+    tc_mbar_init(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+
+  // this thread's voxel: row `tid` of the A tile and lane `tid` of the accumulator
+  const long long v = (long long)blockIdx.x * TC_M + tid;
+  const bool valid = v < voxels;
+  long long t = valid ? v : 0;
+  const int x = (int)(t % g.w);
+  t /= g.w;
+  const int y = (int)(t % g.h);
+  t /= g.h;
+  const int z = (int)(t % g.d);
+  const uint32_t a_row = (uint32_t)((tid & 7) * 16 + (tid >> 3) * 128);
+  const int kcs = cin / 16, iters = 27 * kcs;
+  constexpr uint32_t IDESC = umma_idesc_bf16(TC_M, COUT);
+  uint32_t parity[2] = {0u, 0u};
+  bool ok = true;
+  int issued = 0;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (int it = 0; it < iters; it++) {
+    const int s = it & 1;
+    bool waited = true;
+    if (it >= 2) {  // the MMA of iteration it-2 read this stage
+      waited = tc_mbar_wait(&bar[s], parity[s]);
+      parity[s] ^= 1u;
+    }
+    const int tap = it / kcs, kc = it - tap * kcs;
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    uint4 a0 = zero, a1 = zero;
+    const int xx = x + dx, yy = y + dy, zz = z + dz;
+    if (valid && xx >= 0 && xx < g.w && yy >= 0 && yy < g.h && zz >= 0 && zz < g.d) {
+      const long long nb = v + dx + (long long)g.w * (dy + (long long)g.h * dz);
+      const uint4* src = reinterpret_cast<const uint4*>(in + nb * cin + kc * 16);
+      a0 = __ldg(src);
+      a1 = __ldg(src + 1);
+    }
+    *reinterpret_cast<uint4*>(sA[s] + a_row) = a0;
+    *reinterpret_cast<uint4*>(sA[s] + A_LBO + a_row) = a1;
+    for (int r = tid; r < COUT * 2; r += TC_M) {
+      const int co = r >> 1, kh = r & 1;
+      const uint4 val = __ldg(reinterpret_cast<const uint4*>(w + ((long long)tap * COUT + co) * cin + kc * 16 + kh * 8));
+      *reinterpret_cast<uint4*>(sB[s] + kh * B_LBO + (co & 7) * 16 + (co >> 3) * 128) = val;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tensor core reads through the async proxy
+    if (!__syncthreads_and(waited)) {  // a wait gave up somewhere: stop issuing (block-uniform)
+      ok = false;
+      break;
+    }
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint64_t adesc = umma_desc(smem_addr(sA[s]), A_LBO, 128);
+      const uint64_t bdesc = umma_desc(smem_addr(sB[s]), B_LBO, 128);
+      const uint32_t acc = it > 0 ? 1u : 0u, mask0 = 0u;
+      asm volatile(
+          "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+          " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
+          "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(acc), "r"(mask0)
+          : "memory");
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&bar[s]))
+                   : "memory");
+    }
+    issued = it + 1;
+  }
+  // the last commit tracks every MMA issued before it
+  bool done = true;
+  if (issued > 0) done = tc_mbar_wait(&bar[(issued - 1) & 1], parity[(issued - 1) & 1]);
+  ok = __syncthreads_and(ok && done) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok && valid) {
+    uint32_t* o32 = reinterpret_cast<uint32_t*>(out + v * COUT);
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 8) {
+      uint32_t r[8];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float f[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        f[k] = __uint_as_float(r[k]) + (bias ? bias[c0 + k] : 0.f);
+        if (relu) f[k] = fmaxf(f[k], 0.f);
+      }
+      const uint4 packed = make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]),
+                                      pack_bf16(f[6], f[7]));
+      *reinterpret_cast<uint4*>(o32 + c0 / 2) = packed;
+    }
+  } else if (ok) {
+    // lanes past the last voxel still take part in the warp-wide loads
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 8) {
+      uint32_t r[8];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    }
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
+}
+
 // wt[26 - tap][ci][co] = w[tap][co][ci]
 __global__ void flip_kernel(const bf16* __restrict__ w, bf16* __restrict__ wt, int cin, int cout) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -484,6 +660,23 @@ __global__ void unpack_fields_kernel(const bf16* __restrict__ y, float* __restri
   }
 }
 
+int g_engine = 0;  // forward convolutions: 0 = mma.sync warp tiles, 1 = tcgen05
+__device__ int g_tc_err;  // set by a tcgen05 kernel whose wait gave up
+
+// Device address of g_tc_err, looked up once per device (host code cannot use the
+// symbol itself as a device address).
+int* tc_err_ptr() {
+  static int* ptrs[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_tc_err) != cudaSuccess) return nullptr;
+    ptrs[dev] = (int*)p;
+  }
+  return ptrs[dev];
+}
+
 unsigned blocks_for(long long count, int per) { return (unsigned)((count + per - 1) / per); }
 
 bool geo_ok(int n, int d, int h, int w) { return n > 0 && d > 0 && h > 0 && w > 0; }
@@ -507,6 +700,21 @@ int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* ou
   const bf16* I = (const bf16*)in;
   const bf16* W = (const bf16*)w;
   bf16* O = (bf16*)out;
+  if (g_engine == 1) {
+    int* err = tc_err_ptr();
+    if (!err) return fail("nn_conv3d_fwd: no device address for the error word");
+    const long long vox = (long long)n * d * h * wd;
+    const unsigned tgrid = blocks_for(vox, TC_M);
+    switch (cout) {
+      case 16: conv_fwd_tc_kernel<16><<<tgrid, TC_M, 0, s>>>(I, W, bias, O, g, cin, relu, vox, err); break;
+      case 32: conv_fwd_tc_kernel<32><<<tgrid, TC_M, 0, s>>>(I, W, bias, O, g, cin, relu, vox, err); break;
+      case 48: conv_fwd_tc_kernel<48><<<tgrid, TC_M, 0, s>>>(I, W, bias, O, g, cin, relu, vox, err); break;
+      case 64: conv_fwd_tc_kernel<64><<<tgrid, TC_M, 0, s>>>(I, W, bias, O, g, cin, relu, vox, err); break;
+      case 96: conv_fwd_tc_kernel<96><<<tgrid, TC_M, 0, s>>>(I, W, bias, O, g, cin, relu, vox, err); break;
+      default: return fail("nn_conv3d_fwd: Cout %d not in {16, 32, 48, 64, 96}", cout);
+    }
+    return launched("nn_conv3d_fwd (tcgen05)");
+  }
   switch (cout) {
     case 16: conv_fwd_kernel<2><<<grid, 128, 0, s>>>(I, W, bias, O, g, cin, relu, tiles); break;
     case 32: conv_fwd_kernel<4><<<grid, 128, 0, s>>>(I, W, bias, O, g, cin, relu, tiles); break;
@@ -516,6 +724,29 @@ int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* ou
     default: return fail("nn_conv3d_fwd: Cout %d not in {16, 32, 48, 64, 96}", cout);
   }
   return launched("nn_conv3d_fwd");
+}
+
+int32_t nn_set_conv_engine(int32_t engine) {
+  if (engine != 0 && engine != 1) return fail("nn_set_conv_engine: engine must be 0 (mma.sync) or 1 (tcgen05)");
+  const int prev = g_engine;
+  g_engine = engine;
+  g_err.clear();
+  return prev;
+}
+
+int32_t nn_tc_status(void* stream) {
+  int* err = tc_err_ptr();
+  if (!err) return fail("nn_tc_status: no device address for the error word");
+  int h = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return launched("nn_tc_status");
+  if (h) {
+    cudaMemsetAsync(err, 0, sizeof(int), s);
+    return fail("a tcgen05 convolution gave up waiting for its MMA (error word %d)", h);
+  }
+  return 0;
 }
 
 int32_t nn_conv3d_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream) {

@@ -212,7 +212,7 @@ class Stepper:
 
 
 def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int = 30000, tol: float = 1e-6,
-             group: int = 64, log=print, augment: bool = True):
+             group: int = 64, log=print, augment: bool = False):
     """Steady states of the cases, kept on the GPU: BF16 features (n, NZ, NY, NX, 16),
     FP32 targets (n, NZ, NY, NX, 4), fluid masks, fluid counts, and the record of
     each run (steps, stability).  With `augment`, each steady state also enters in its
@@ -297,7 +297,7 @@ def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3,
     return hist
 
 
-def predict(model, params: Sequence[dict], mirror_average: bool = True):
+def predict(model, params: Sequence[dict], mirror_average: bool = False):
     """Equilibrium initial fields (rho, u, v, w as FP64 host arrays) per case; with
     `mirror_average` the network sees the case in its four mirror images (one batch)
     and the predictions, mapped back, are averaged."""
@@ -374,6 +374,8 @@ def main(argv=None):
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--drag-tol", type=float, default=1e-5)
     ap.add_argument("--fallback", type=float, default=0.05)
+    ap.add_argument("--augment", action="store_true", help="train on the three mirror images of every state too")
+    ap.add_argument("--mirror-average", action="store_true", help="average the prediction over the four mirror images")
     ap.add_argument("--out", default="warmstart_out")
     args = ap.parse_args(argv)
     import torch
@@ -401,7 +403,7 @@ def _run(args, stream, out, log):
     t0 = time.perf_counter()
     train_seeds = list(range(args.train))
     held = list(range(100000, 100000 + args.heldout))
-    X, T, M, counts, rec = generate(train_seeds, 0, stream, args.max_steps, args.tol, log=log)
+    X, T, M, counts, rec = generate(train_seeds, 0, stream, args.max_steps, args.tol, log=log, augment=args.augment)
     log(f"training set: {X.shape[0]} steady states of {len(train_seeds)} ({time.perf_counter() - t0:.0f} s)")
     model = UNet3D(16, 0, stream, seed=0)
     t1 = time.perf_counter()
@@ -414,7 +416,7 @@ def _run(args, stream, out, log):
     # warm: inference (timed) + runs; rest: runs
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    init = predict(model, params)
+    init = predict(model, params, mirror_average=args.mirror_average)
     e1.record(stream)
     e1.synchronize()
     infer_ms = e0.elapsed_time(e1)

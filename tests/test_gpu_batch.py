@@ -66,10 +66,9 @@ def test_batch_step_matches_single_domains(gpu, storage):
 
 
 def _row32(cls, k):
-    """Rows of 32 cells, periodic along x: single launches (32 x 4 blocks) and the batch
-    (128-cell items in row order) put the same cells in the same warps, so the results
-    must agree bit for bit.  (With a non-periodic x axis the batch orders face columns
-    last, which regroups warps.)"""
+    """Rows of 32 cells: single launches (32 x 4 blocks) and the batch (128-cell items in
+    row order) put the same cells in the same warps, so the results must agree bit for
+    bit."""
     ny, nz = (8, 8) if k == 0 else (12, 5)
     faces = ("periodic", "periodic", "wall", "wall", "wall", "wall")
     d = cls(32, ny, nz, collision="BGK", storage="fp64", faces=faces, omega_p=1.0 / (0.6 + 0.1 * k),

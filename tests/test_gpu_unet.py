@@ -45,9 +45,17 @@ def _host(t, ops):
 SHAPE = (2, 3, 5, 32)
 
 
+@pytest.fixture(params=["mma", "tcgen05"])
+def engine(request, gpu):
+    prev = N.set_conv_engine(request.param)
+    yield request.param
+    N.tc_status()
+    N.set_conv_engine(prev)
+
+
 @pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 64), (64, 64), (96, 32), (48, 16), (32, 48), (64, 96)])
 @pytest.mark.parametrize("relu", [False, True])
-def test_conv_forward(ops, cin, cout, relu):
+def test_conv_forward(ops, engine, cin, cout, relu):
     import torch
 
     rng = np.random.default_rng(cin * 1000 + cout)
@@ -97,7 +105,7 @@ def test_conv_weight_gradient_many_chunks(ops):
 
 
 @pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 64), (96, 32), (48, 16)])
-def test_conv_data_gradient(ops, cin, cout):
+def test_conv_data_gradient(ops, engine, cin, cout):
     import torch
 
     rng = np.random.default_rng(11 + cin + cout)
@@ -151,7 +159,7 @@ def _net_case(seed=0, shape=(1, 8, 8, 64)):
     return params, x, target, mask, cw
 
 
-def test_network_forward_backward_vs_oracle(gpu):
+def test_network_forward_backward_vs_oracle(engine):
     import torch
 
     params, x, target, mask, cw = _net_case()
