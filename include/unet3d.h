@@ -35,8 +35,9 @@ int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* ou
                       int32_t h, int32_t wd, int32_t cin, int32_t cout, int32_t relu, void* stream);
 /* Engine of nn_conv3d_fwd (and so of the data gradient): 0 = mma.sync warp tiles
  * (FP32 accumulation in registers), 1 = tcgen05 (128-voxel CTA tiles, operands in
- * shared memory, FP32 accumulator in tensor memory).  Returns the previous engine, or
- * nonzero with nn_last_error() for an unknown engine.  Process-wide. */
+ * shared memory, FP32 accumulator in tensor memory), 2 = per layer (default: tcgen05
+ * for Cout >= 32, warp tiles for Cout = 16).  Returns the previous engine, or -1 with
+ * nn_last_error() for an unknown engine.  Process-wide. */
 int32_t nn_set_conv_engine(int32_t engine);
 /* Blocking: nonzero (and cleared) when a tcgen05 convolution gave up waiting for its
  * matrix multiply since the last call; its output is then not valid. */

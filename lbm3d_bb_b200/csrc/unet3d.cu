@@ -660,7 +660,10 @@ __global__ void unpack_fields_kernel(const bf16* __restrict__ y, float* __restri
   }
 }
 
-int g_engine = 0;  // forward convolutions: 0 = mma.sync warp tiles, 1 = tcgen05
+// forward convolutions: 0 = mma.sync warp tiles, 1 = tcgen05, 2 = per layer (tcgen05 when
+// Cout >= 32: with Cout = 16 one 128-voxel gather feeds too small an MMA and the warp
+// tiles are faster, measured on B200)
+int g_engine = 2;
 __device__ int g_tc_err;  // set by a tcgen05 kernel whose wait gave up
 
 // Device address of g_tc_err, looked up once per device (host code cannot use the
@@ -700,7 +703,7 @@ int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* ou
   const bf16* I = (const bf16*)in;
   const bf16* W = (const bf16*)w;
   bf16* O = (bf16*)out;
-  if (g_engine == 1) {
+  if (g_engine == 1 || (g_engine == 2 && cout >= 32)) {
     int* err = tc_err_ptr();
     if (!err) return fail("nn_conv3d_fwd: no device address for the error word");
     const long long vox = (long long)n * d * h * wd;
@@ -727,7 +730,10 @@ int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* ou
 }
 
 int32_t nn_set_conv_engine(int32_t engine) {
-  if (engine != 0 && engine != 1) return fail("nn_set_conv_engine: engine must be 0 (mma.sync) or 1 (tcgen05)");
+  if (engine < 0 || engine > 2) {
+    fail("nn_set_conv_engine: engine must be 0 (mma.sync), 1 (tcgen05) or 2 (per layer)");
+    return -1;
+  }
   const int prev = g_engine;
   g_engine = engine;
   g_err.clear();

@@ -77,13 +77,14 @@ def exported_symbols() -> list[str]:
             "nn_from_bf16"]
 
 
-ENGINES = {"mma": 0, "tcgen05": 1}
+ENGINES = {"mma": 0, "tcgen05": 1, "auto": 2}
 
 
 def set_conv_engine(name: str) -> str:
-    """Selects the forward-convolution kernels ('mma' or 'tcgen05'); returns the previous one."""
+    """Selects the forward-convolution kernels ('mma', 'tcgen05' or 'auto': tcgen05 for
+    Cout >= 32); returns the previous one."""
     prev = lib().nn_set_conv_engine(ENGINES[name])
-    if prev not in (0, 1):
+    if prev not in (0, 1, 2):
         raise NnError((lib().nn_last_error() or b"").decode(errors="replace"))
     return {v: k for k, v in ENGINES.items()}[prev]
 
@@ -338,3 +339,39 @@ class UNet3D:
         z = np.load(path)
         params = {k: z[k] for k in z.files if k != "width"}
         return cls(int(z["width"]), device, stream, params)
+
+
+def _conv_cli(argv=None) -> None:
+    """Times repeated launches of one convolution layer (zero tensors):
+    python -m lbm3d_bb_b200.unet --engine tcgen05 --shape 2,64,64,128 --cin 48 --cout 16 --launches 4"""
+    import argparse
+
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--engine", default="auto", choices=sorted(ENGINES))
+    ap.add_argument("--shape", default="2,64,64,128", help="n,d,h,w")
+    ap.add_argument("--cin", type=int, default=48)
+    ap.add_argument("--cout", type=int, default=16)
+    ap.add_argument("--launches", type=int, default=4)
+    args = ap.parse_args(argv)
+    n, d, h, w = (int(v) for v in args.shape.split(","))
+    set_conv_engine(args.engine)
+    ops = Ops()
+    x = torch.zeros((n, d, h, w, args.cin), dtype=torch.bfloat16, device="cuda")
+    y = torch.empty((n, d, h, w, args.cout), dtype=torch.bfloat16, device="cuda")
+    wt = torch.zeros((27, args.cout, args.cin), dtype=torch.bfloat16, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.launches):
+        ops.conv(x, wt, None, y, (n, d, h, w), args.cin, args.cout, True)
+    e1.record()
+    e1.synchronize()
+    tc_status()
+    ms = e0.elapsed_time(e1) / args.launches
+    flops = 2.0 * n * d * h * w * 27 * args.cin * args.cout
+    print(f"{args.engine}: {ms:.3f} ms per launch, {flops / (ms * 1e-3) / 1e12:.1f} TFLOP/s")
+
+
+if __name__ == "__main__":
+    _conv_cli()

@@ -45,7 +45,7 @@ def _host(t, ops):
 SHAPE = (2, 3, 5, 32)
 
 
-@pytest.fixture(params=["mma", "tcgen05"])
+@pytest.fixture(params=["mma", "tcgen05", "auto"])
 def engine(request, gpu):
     prev = N.set_conv_engine(request.param)
     yield request.param
