@@ -34,11 +34,17 @@ const char* nn_last_error(void);
 int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* out, int32_t n, int32_t d,
                       int32_t h, int32_t wd, int32_t cin, int32_t cout, int32_t relu, void* stream);
 /* Engine of nn_conv3d_fwd (and so of the data gradient): 0 = mma.sync warp tiles
- * (FP32 accumulation in registers), 1 = tcgen05 (128-voxel CTA tiles, operands in
- * shared memory, FP32 accumulator in tensor memory), 2 = per layer (default: tcgen05
- * for Cout >= 32, warp tiles for Cout = 16).  Returns the previous engine, or -1 with
- * nn_last_error() for an unknown engine.  Process-wide. */
+ * (FP32 accumulation in registers); 1 = tcgen05 (128-voxel CTA tiles gathered into
+ * shared memory by the threads, FP32 accumulator in tensor memory); 2 = per layer
+ * (default: tcgen05 for Cout >= 32, warp tiles for Cout = 16); 3 = tcgen05 with the tiles
+ * loaded by TMA (5-D tensor map, zero fill for the halo) where nn_conv_uses_tma says so,
+ * else as 1.  Returns the previous engine, or -1 with nn_last_error() for an unknown
+ * engine.  Process-wide. */
 int32_t nn_set_conv_engine(int32_t engine);
+/* 1 when a forward convolution of this shape runs the TMA-fed tcgen05 kernel under the
+ * current engine (engine 3, tiles of 128 voxels = whole rows or part of one row, a
+ * tensor-map encoder from the driver), 0 when it runs one of the other kernels. */
+int32_t nn_conv_uses_tma(int32_t h, int32_t wd, int32_t cin, int32_t cout);
 /* Blocking: nonzero (and cleared) when a tcgen05 convolution gave up waiting for its
  * matrix multiply since the last call; its output is then not valid. */
 int32_t nn_tc_status(void* stream);

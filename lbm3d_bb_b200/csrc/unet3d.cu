@@ -16,8 +16,10 @@
 // it stages 64-voxel slabs of dY and of the shifted input in shared memory and
 // feeds the MMAs with transposing ldmatrix loads; partial sums go to the FP32
 // gradient with one atomic add per element and block.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched at run time)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
 #include <cstdarg>
@@ -315,6 +317,164 @@ __global__ void __launch_bounds__(TC_M) conv_fwd_tc_kernel(const bf16* __restric
     }
   }
   if (!ok && tid == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
+}
+
+// ---- tcgen05 convolution fed by TMA --------------------------------------------------
+// Same tiling as conv_fwd_tc_kernel, but the A tile of a tap is a TMA box of the
+// activations: a 5-D tensor map over (C, W, H, D, N) with box {8, min(W,128),
+// 128 / min(W,128), 1, 1} lands in shared memory as 128 rows of 16 bytes — exactly the
+// K-major interleaved core-matrix layout (8-row groups 128 bytes apart) — and its
+// out-of-range rows (the 1-voxel halo at the box faces) are filled with zeros by the
+// copy engine.  Two boxes (channel halves) per tap and 16-channel slice, two more for the
+// weights; one thread runs the whole pipeline (TMA issue into a ring of stages, MMA issue
+// when a stage's bytes have landed, commit that frees the stage), so no CTA barrier sits
+// in the K loop.  Every wait is bounded.
+constexpr int TMA_STAGES = 4;
+
+__device__ __forceinline__ void tc_mbar_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_addr(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <int COUT>
+__global__ void __launch_bounds__(TC_M) conv_fwd_tma_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                            const __grid_constant__ CUtensorMap wmap,
+                                                            const float* __restrict__ bias, bf16* __restrict__ out,
+                                                            const Geo g, const int cin, const int relu, int* err) {
+  constexpr int NCOL = COUT <= 32 ? 32 : (COUT <= 64 ? 64 : 128);
+  constexpr uint32_t A_LBO = TC_M * 16, B_LBO = COUT * 16;
+  constexpr uint32_t STAGE_BYTES = 2 * A_LBO + 2 * B_LBO;
+  __shared__ __align__(128) uint8_t sbuf[TMA_STAGES][STAGE_BYTES];
+  __shared__ __align__(8) uint64_t full[TMA_STAGES], empty[TMA_STAGES];
+  __shared__ uint32_t tmem_base;
+  __shared__ int ok_s;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
+                 "r"(NCOL)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < TMA_STAGES; s++) {
+      tc_mbar_init(&full[s]);
+      tc_mbar_init(&empty[s]);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  // tile -> (n, z, y0, x0): 128 voxels = part of one row (W >= 128) or 128/W whole rows
+  const int bw = g.w < TC_M ? g.w : TC_M, bh = TC_M / bw;
+  const int tiles_x = g.w / bw, tiles_y = g.h / bh;
+  long long tile = blockIdx.x;
+  const int tx = (int)(tile % tiles_x);
+  tile /= tiles_x;
+  const int ty = (int)(tile % tiles_y);
+  tile /= tiles_y;
+  const int z = (int)(tile % g.d), n = (int)(tile / g.d);
+  const int x0 = tx * bw, y0 = ty * bh;
+  const int kcs = cin / 16, iters = 27 * kcs;
+  constexpr uint32_t IDESC = umma_idesc_bf16(TC_M, COUT);
+  if (tid == 0) {
+    bool ok = true;
+    uint32_t fpar[TMA_STAGES] = {}, epar[TMA_STAGES] = {};
+    int issued_mma = 0;
+    for (int it = 0; it < iters + TMA_STAGES - 1 && ok; it++) {
+      if (it < iters) {  // producer: stage it % S
+        const int s = it % TMA_STAGES;
+        if (it >= TMA_STAGES) {  // the MMA of it - S must have released the stage
+          ok = tc_mbar_wait(&empty[s], epar[s]);
+          epar[s] ^= 1u;
+          if (!ok) break;
+        }
+        const int tap = it / kcs, kc = it - tap * kcs;
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        uint8_t* st = sbuf[s];
+        tc_mbar_expect(&full[s], STAGE_BYTES);
+        tma_load_5d(st, &xmap, kc * 16, x0 + dx, y0 + dy, z + dz, n, &full[s]);
+        tma_load_5d(st + A_LBO, &xmap, kc * 16 + 8, x0 + dx, y0 + dy, z + dz, n, &full[s]);
+        tma_load_3d(st + 2 * A_LBO, &wmap, kc * 16, 0, tap, &full[s]);
+        tma_load_3d(st + 2 * A_LBO + B_LBO, &wmap, kc * 16 + 8, 0, tap, &full[s]);
+      }
+      const int j = it - (TMA_STAGES - 1);
+      if (j >= 0) {  // consumer: MMA of iteration j
+        const int s = j % TMA_STAGES;
+        ok = tc_mbar_wait(&full[s], fpar[s]);
+        fpar[s] ^= 1u;
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint64_t adesc = umma_desc(smem_addr(sbuf[s]), A_LBO, 128);
+        const uint64_t bdesc = umma_desc(smem_addr(sbuf[s] + 2 * A_LBO), B_LBO, 128);
+        const uint32_t acc = j > 0 ? 1u : 0u, mask0 = 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
+            "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(acc), "r"(mask0)
+            : "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&empty[s]))
+                     : "memory");
+        issued_mma = j + 1;
+      }
+    }
+    // the last commit tracks every MMA before it; drain the ring (bounded) either way
+    if (issued_mma > 0) {
+      const int s = (issued_mma - 1) % TMA_STAGES;
+      const bool done = tc_mbar_wait(&empty[s], epar[s]);
+      ok = ok && done;
+    }
+    ok_s = ok && issued_mma == iters ? 1 : 0;
+  }
+  __syncthreads();
+  const bool ok = ok_s != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int r = tid;  // accumulator lane = tile row = voxel
+    const int x = x0 + (r % bw), y = y0 + r / bw;
+    const long long v = (((long long)n * g.d + z) * g.h + y) * g.w + x;
+    uint32_t* o32 = reinterpret_cast<uint32_t*>(out + v * COUT);
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 8) {
+      uint32_t q[8];
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                   : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7])
+                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float f[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        f[k] = __uint_as_float(q[k]) + (bias ? bias[c0 + k] : 0.f);
+        if (relu) f[k] = fmaxf(f[k], 0.f);
+      }
+      *reinterpret_cast<uint4*>(o32 + c0 / 2) =
+          make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
+    }
+  } else if (tid == 0) {
+    atomicExch(err, 1);
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
@@ -660,10 +820,33 @@ __global__ void unpack_fields_kernel(const bf16* __restrict__ y, float* __restri
   }
 }
 
-// forward convolutions: 0 = mma.sync warp tiles, 1 = tcgen05, 2 = per layer (tcgen05 when
-// Cout >= 32: with Cout = 16 one 128-voxel gather feeds too small an MMA and the warp
-// tiles are faster, measured on B200)
+// forward convolutions: 0 = mma.sync warp tiles, 1 = tcgen05 with thread-gathered tiles,
+// 2 = per layer (tcgen05 when Cout >= 32: with Cout = 16 one 128-voxel gather feeds too
+// small an MMA and the warp tiles are faster, measured on B200), 3 = tcgen05 with
+// TMA-fed tiles where the shape allows (slower on B200 with these 16-byte-wide boxes:
+// the copy engine issues one request per 16-byte row)
 int g_engine = 2;
+
+// cuTensorMapEncodeTiled from the driver (fetched once, no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// The TMA-fed kernel takes tiles of 128 voxels that are whole rows or part of one row.
+bool tma_tiles_fit(int h, int w) {
+  if (w >= TC_M) return w % TC_M == 0;
+  return TC_M % w == 0 && h % (TC_M / w) == 0;
+}
 __device__ int g_tc_err;  // set by a tcgen05 kernel whose wait gave up
 
 // Device address of g_tc_err, looked up once per device (host code cannot use the
@@ -703,9 +886,39 @@ int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* ou
   const bf16* I = (const bf16*)in;
   const bf16* W = (const bf16*)w;
   bf16* O = (bf16*)out;
-  if (g_engine == 1 || (g_engine == 2 && cout >= 32)) {
+  if (g_engine == 1 || g_engine == 3 || (g_engine == 2 && cout >= 32)) {
     int* err = tc_err_ptr();
     if (!err) return fail("nn_conv3d_fwd: no device address for the error word");
+    PFN_cuTensorMapEncodeTiled_v12000 enc = g_engine == 3 ? tensor_map_encoder() : nullptr;
+    if (enc && tma_tiles_fit(h, wd) && cin % 16 == 0) {
+      CUtensorMap xmap, wmap;
+      const cuuint64_t xdim[5] = {(cuuint64_t)cin, (cuuint64_t)wd, (cuuint64_t)h, (cuuint64_t)d, (cuuint64_t)n};
+      const cuuint64_t xstr[4] = {(cuuint64_t)cin * 2, (cuuint64_t)wd * cin * 2, (cuuint64_t)h * wd * cin * 2,
+                                  (cuuint64_t)d * h * wd * cin * 2};
+      const int bw = wd < TC_M ? wd : TC_M;
+      const cuuint32_t xbox[5] = {8, (cuuint32_t)bw, (cuuint32_t)(TC_M / bw), 1, 1};
+      const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+      const cuuint64_t wdim[3] = {(cuuint64_t)cin, (cuuint64_t)cout, 27};
+      const cuuint64_t wstr[2] = {(cuuint64_t)cin * 2, (cuuint64_t)cout * cin * 2};
+      const cuuint32_t wbox[3] = {8, (cuuint32_t)cout, 1};
+      CUresult r1 = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(in), xdim, xstr, xbox, one,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      CUresult r2 = enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(w), wdim, wstr, wbox, one,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) return fail("nn_conv3d_fwd: tensor map encoding failed (%d, %d)", (int)r1, (int)r2);
+      const unsigned tgrid = (unsigned)((long long)n * d * (h / (TC_M / bw)) * (wd / bw));
+      switch (cout) {
+        case 16: conv_fwd_tma_kernel<16><<<tgrid, TC_M, 0, s>>>(xmap, wmap, bias, O, g, cin, relu, err); break;
+        case 32: conv_fwd_tma_kernel<32><<<tgrid, TC_M, 0, s>>>(xmap, wmap, bias, O, g, cin, relu, err); break;
+        case 48: conv_fwd_tma_kernel<48><<<tgrid, TC_M, 0, s>>>(xmap, wmap, bias, O, g, cin, relu, err); break;
+        case 64: conv_fwd_tma_kernel<64><<<tgrid, TC_M, 0, s>>>(xmap, wmap, bias, O, g, cin, relu, err); break;
+        case 96: conv_fwd_tma_kernel<96><<<tgrid, TC_M, 0, s>>>(xmap, wmap, bias, O, g, cin, relu, err); break;
+        default: return fail("nn_conv3d_fwd: Cout %d not in {16, 32, 48, 64, 96}", cout);
+      }
+      return launched("nn_conv3d_fwd (tcgen05, TMA)");
+    }
     const long long vox = (long long)n * d * h * wd;
     const unsigned tgrid = blocks_for(vox, TC_M);
     switch (cout) {
@@ -730,14 +943,19 @@ int32_t nn_conv3d_fwd(const void* in, const void* w, const float* bias, void* ou
 }
 
 int32_t nn_set_conv_engine(int32_t engine) {
-  if (engine < 0 || engine > 2) {
-    fail("nn_set_conv_engine: engine must be 0 (mma.sync), 1 (tcgen05) or 2 (per layer)");
+  if (engine < 0 || engine > 3) {
+    fail("nn_set_conv_engine: engine must be 0 (mma.sync), 1 (tcgen05), 2 (per layer) or 3 (tcgen05, TMA-fed)");
     return -1;
   }
   const int prev = g_engine;
   g_engine = engine;
   g_err.clear();
   return prev;
+}
+
+int32_t nn_conv_uses_tma(int32_t h, int32_t wd, int32_t cin, int32_t cout) {
+  (void)cout;
+  return (g_engine == 3 && tensor_map_encoder() && tma_tiles_fit(h, wd) && cin % 16 == 0) ? 1 : 0;
 }
 
 int32_t nn_tc_status(void* stream) {

@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
         "nn_features_ellipsoid": (i32, [vp, i32, i32, i32, vp, vp, vp, f32, vp]),
         "nn_unpack_fields": (i32, [vp, vp, i32, i32, i32, i32, i32, i32, f32, i32, vp]),
         "nn_set_conv_engine": (i32, [i32]),
+        "nn_conv_uses_tma": (i32, [i32, i32, i32, i32]),
         "nn_tc_status": (i32, [vp]),
         "nn_to_bf16": (i32, [vp, vp, i64, vp]),
         "nn_from_bf16": (i32, [vp, vp, i64, vp]),
@@ -71,20 +72,20 @@ def lib() -> C.CDLL:
 
 
 def exported_symbols() -> list[str]:
-    return ["nn_abi_version", "nn_last_error", "nn_set_conv_engine", "nn_tc_status", "nn_conv3d_fwd", "nn_conv3d_flip", "nn_conv3d_bwd_weight",
+    return ["nn_abi_version", "nn_last_error", "nn_set_conv_engine", "nn_conv_uses_tma", "nn_tc_status", "nn_conv3d_fwd", "nn_conv3d_flip", "nn_conv3d_bwd_weight",
             "nn_bias_grad", "nn_relu_bwd", "nn_pool2", "nn_pool2_bwd", "nn_up2_concat", "nn_up2_concat_bwd",
             "nn_mse", "nn_adam", "nn_diff_norms", "nn_features_ellipsoid", "nn_unpack_fields", "nn_to_bf16",
             "nn_from_bf16"]
 
 
-ENGINES = {"mma": 0, "tcgen05": 1, "auto": 2}
+ENGINES = {"mma": 0, "tcgen05": 1, "auto": 2, "tcgen05-tma": 3}
 
 
 def set_conv_engine(name: str) -> str:
-    """Selects the forward-convolution kernels ('mma', 'tcgen05' or 'auto': tcgen05 for
-    Cout >= 32); returns the previous one."""
+    """Selects the forward-convolution kernels ('mma', 'tcgen05', 'auto': tcgen05 for
+    Cout >= 32, or 'tcgen05-tma'); returns the previous one."""
     prev = lib().nn_set_conv_engine(ENGINES[name])
-    if prev not in (0, 1, 2):
+    if prev not in (0, 1, 2, 3):
         raise NnError((lib().nn_last_error() or b"").decode(errors="replace"))
     return {v: k for k, v in ENGINES.items()}[prev]
 

@@ -45,7 +45,7 @@ def _host(t, ops):
 SHAPE = (2, 3, 5, 32)
 
 
-@pytest.fixture(params=["mma", "tcgen05", "auto"])
+@pytest.fixture(params=["mma", "tcgen05", "auto", "tcgen05-tma"])
 def engine(request, gpu):
     prev = N.set_conv_engine(request.param)
     yield request.param
@@ -70,6 +70,29 @@ def test_conv_forward(ops, engine, cin, cout, relu):
     got = _host(y, ops)
     assert rel_l2(got, U.to_bf16(ref)) <= 3e-3  # BF16 output rounding of FP32 vs FP64 sums
     assert rel_l2(got, ref) <= 5e-3
+
+
+@pytest.mark.parametrize("shape", [(2, 3, 8, 32), (1, 2, 2, 128), (1, 2, 4, 64), (1, 3, 16, 16), (1, 2, 3, 256)])
+@pytest.mark.parametrize("cin,cout", [(16, 32), (32, 64), (96, 32), (16, 96), (48, 48), (64, 16)])
+def test_conv_forward_tma_fed(ops, shape, cin, cout):
+    """Shapes whose 128-voxel tiles are whole rows or part of one row take the TMA-fed
+    tcgen05 kernel (halo from the copy engine's zero fill)."""
+    import torch
+
+    prev = N.set_conv_engine("tcgen05-tma")
+    try:
+        assert N.lib().nn_conv_uses_tma(shape[2], shape[3], cin, cout) == 1
+        rng = np.random.default_rng(sum(shape) + cin + cout)
+        x = U.to_bf16(rng.standard_normal(shape + (cin,)))
+        w = U.to_bf16(rng.standard_normal((27, cout, cin)) / np.sqrt(27 * cin))
+        b = rng.standard_normal(cout) * 0.1
+        y = torch.empty(shape + (cout,), dtype=torch.bfloat16, device="cuda")
+        ops.conv(_dev(x, ops), _dev(w, ops), _dev(b, ops, False), y, shape, cin, cout, True)
+        N.tc_status()
+        ref = np.maximum(U.conv(x, w, b), 0)
+        assert rel_l2(_host(y, ops), ref) <= 5e-3
+    finally:
+        N.set_conv_engine(prev)
 
 
 @pytest.mark.parametrize("cin,cout", [(16, 16), (32, 16), (48, 16), (96, 32), (16, 32), (32, 64), (64, 64)])
