@@ -263,7 +263,7 @@ def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int 
 
 
 def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3, seed: int = 0, log=print,
-          lr_min: float = 1e-5):
+          lr_min: float = 1e-5, weights=CHANNEL_WEIGHTS):
     """Adam on the masked MSE over the GPU-resident data set (shuffled mini-batches
     gathered by index), learning rate decayed from lr to lr_min on a cosine.  Returns
     the per-epoch mean loss."""
@@ -271,7 +271,7 @@ def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3,
 
     dev = model.dev
     n = X.shape[0]
-    cw = torch.tensor(CHANNEL_WEIGHTS, dtype=torch.float32, device=dev)
+    cw = torch.tensor(weights, dtype=torch.float32, device=dev)
     acc = torch.zeros(1, dtype=torch.float64, device=dev)
     rng = np.random.default_rng(seed)
     hist = []
@@ -374,6 +374,7 @@ def main(argv=None):
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--drag-tol", type=float, default=1e-5)
     ap.add_argument("--fallback", type=float, default=0.05)
+    ap.add_argument("--rho-weight", type=float, default=1.0, help="loss weight of the density channel")
     ap.add_argument("--augment", action="store_true", help="train on the three mirror images of every state too")
     ap.add_argument("--mirror-average", action="store_true", help="average the prediction over the four mirror images")
     ap.add_argument("--out", default="warmstart_out")
@@ -407,7 +408,8 @@ def _run(args, stream, out, log):
     log(f"training set: {X.shape[0]} steady states of {len(train_seeds)} ({time.perf_counter() - t0:.0f} s)")
     model = UNet3D(16, 0, stream, seed=0)
     t1 = time.perf_counter()
-    hist = train(model, X, T, M, counts, args.epochs, args.batch, args.lr, log=log)
+    hist = train(model, X, T, M, counts, args.epochs, args.batch, args.lr, log=log,
+                 weights=(args.rho_weight,) + CHANNEL_WEIGHTS[1:])
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t1
     model.save(out / "unet_c5.npz")
