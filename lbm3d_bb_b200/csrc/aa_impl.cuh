@@ -665,6 +665,193 @@ __global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __gr
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
+// ---- pair kernel (fully periodic boxes, nx a multiple of 128) ---------------------------
+// One thread updates the two x-adjacent cells (x0, x0+1), x0 even.  The two cells' slots
+// of a direction are adjacent and aligned to twice the element size whenever the
+// direction has no x component (all 19 in the even phase, 9 in the odd phase): those
+// move as one two-element word (half2 / float2 / double2); the x-shifted ones move as
+// two elements.  Addressing and control are shared by the pair and every thread keeps
+// more loads in flight.  Warps that meet a non-static boundary rerun both cells on the
+// general path; a solid cell's own slots are never read by anyone, so an even-phase
+// two-element store may overwrite them.
+template <class S>
+struct Pair2;
+template <>
+struct Pair2<__half> {
+  static __device__ __forceinline__ void ld(const __half* p, float& a, float& b) {
+    const __half2 h = *reinterpret_cast<const __half2*>(p);
+    a = __low2float(h);
+    b = __high2float(h);
+  }
+  static __device__ __forceinline__ void st(__half* p, float a, float b) {
+    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
+  }
+};
+template <>
+struct Pair2<float> {
+  static __device__ __forceinline__ void ld(const float* p, float& a, float& b) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    a = v.x;
+    b = v.y;
+  }
+  static __device__ __forceinline__ void st(float* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+};
+template <>
+struct Pair2<double> {
+  static __device__ __forceinline__ void ld(const double* p, double& a, double& b) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    a = v.x;
+    b = v.y;
+  }
+  static __device__ __forceinline__ void st(double* p, double a, double b) {
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
+  }
+};
+
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__device__ __forceinline__ void pair_cell(const AAParams& p, const typename SP::C* f, typename SP::C* pst) {
+  using C = typename SP::C;
+  const Coll<C> k{C(p.omega_p), C(p.omega_m), C(p.gacc[0]), C(p.gacc[1]), C(p.gacc[2])};
+  const C rho0 = C(p.rho0);
+  C rho, ux, uy, uz;
+  moments<C, FORCE, SP::DEV>(f, k, rho, ux, uy, uz, rho0);
+  collide<C, TRT, FORCE, SP::DEV>(f, pst, k, rho, ux, uy, uz, rho0);
+}
+
+template <class SP>
+__device__ __forceinline__ void pair_links(const AAParams& p, const int x, const int y, const int z, const uint32_t bc,
+                                           const typename SP::C* pst, double* acc) {
+  using C = typename SP::C;
+#pragma unroll
+  for (int d = 0; d < 18; d++) {
+    if (!((bc >> d) & 1u)) continue;
+    const int o = opp(d);
+    const double t = 2.0 * (double)(SP::DEV ? pst[o] + wgt<C>(o) * C(p.rho0) : pst[o]);
+    const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
+    const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
+    const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
+    const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
+    acc[0] += fx;
+    acc[1] += fy;
+    acc[2] += fz;
+    acc[3] += ry * fz - rz * fy;
+    acc[4] += rz * fx - rx * fz;
+    acc[5] += rx * fy - ry * fx;
+  }
+}
+
+template <class SP, bool ODD, bool TRT, bool FORCE>
+__global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_kernel(const __grid_constant__ AAParams p,
+                                                                                typename SP::S* __restrict__ A,
+                                                                                const uint8_t* __restrict__ flags) {
+  using S = typename SP::S;
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = x0 < g.nx && y < g.ny;
+  clear_record(p.zero_next);
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  const long long i0 = inb ? node_index(g, x0, y, z) : 0;
+  const bool coord_fast = inb && (!ODD || (y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1));
+  uint32_t fl0 = F_SOLID, fl1 = F_SOLID;
+  if (inb) {
+    const uint32_t fw = *reinterpret_cast<const unsigned short*>(flags + i0);
+    fl0 = fw & 0xFFu;
+    fl1 = fw >> 8;
+  }
+  const long long fix_lo = x0 == 0 ? (long long)g.nx : 0;            // cell 0 at x = 0
+  const long long fix_hi = x0 + 1 == g.nx - 1 ? (long long)g.nx : 0;  // cell 1 at x = nx - 1
+  C f0[Q], f1[Q];
+  if (coord_fast) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      const long long o = p.off_rd[d];
+      if (!ODD || cx(d) == 0) {
+        Pair2<S>::ld(A + i0 + o, f0[d], f1[d]);
+      } else {
+        f0[d] = ld_fast<SP>(A + i0 + o + (cx(d) == 1 ? fix_lo : 0), d, C(p.rho0));
+        f1[d] = ld_fast<SP>(A + i0 + 1 + o - (cx(d) == -1 ? fix_hi : 0), d, C(p.rho0));
+      }
+    }
+  }
+  const bool solid0 = (fl0 & F_SOLID) != 0, solid1 = (fl1 & F_SOLID) != 0;
+  uint32_t bc0 = 0, bc1 = 0;
+  bool st0 = true, st1 = true;
+  if (!solid0 && (fl0 & F_NEAR)) {
+    const unsigned long long lw = p.links[i0];
+    bc0 = (uint32_t)(lw & 0x3FFFFu);
+    st0 = bc0 == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 && !(fl0 & F_SOLID_PREV);
+  }
+  if (!solid1 && (fl1 & F_NEAR)) {
+    const unsigned long long lw = p.links[i0 + 1];
+    bc1 = (uint32_t)(lw & 0x3FFFFu);
+    st1 = bc1 == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 && !(fl1 & F_SOLID_PREV);
+  }
+  const bool both_solid = solid0 && solid1;
+  const bool fast = coord_fast && st0 && st1;
+  if (__all_sync(0xffffffffu, both_solid || fast)) {
+    if (!both_solid) {
+      if (ODD && (bc0 | bc1)) {  // bounce-back values are kept in the own slots
+#pragma unroll
+        for (int d = 0; d < 18; d++) {
+          if ((bc0 >> d) & 1u) f0[d] = ld_fast<SP>(A + (long long)d * g.plane + i0, d, C(p.rho0));
+          if ((bc1 >> d) & 1u) f1[d] = ld_fast<SP>(A + (long long)d * g.plane + i0 + 1, d, C(p.rho0));
+        }
+      }
+      C p0[Q], p1[Q];
+      if (!solid0) {
+        pair_cell<SP, ODD, TRT, FORCE>(p, f0, p0);
+      } else {
+#pragma unroll
+        for (int d = 0; d < Q; d++) p0[d] = C(0);
+      }
+      if (!solid1) {
+        pair_cell<SP, ODD, TRT, FORCE>(p, f1, p1);
+      } else {
+#pragma unroll
+        for (int d = 0; d < Q; d++) p1[d] = C(0);
+      }
+      const bool plain = !solid0 && !solid1 && !(bc0 | bc1);
+      const C rho0 = C(p.rho0);
+#pragma unroll
+      for (int j = 0; j < Q; j++) {
+        if (!ODD) {  // own slots of both cells: one word
+          Pair2<S>::st(A + (long long)j * g.plane + i0, p0[opp(j)], p1[opp(j)]);
+          continue;
+        }
+        const long long o = p.off_wr[j];
+        const int oj = opp(j);
+        if (cx(j) == 0 && plain) {
+          Pair2<S>::st(A + i0 + o, p0[j], p1[j]);
+          continue;
+        }
+        if (!solid0) {
+          long long a = i0 + o + (cx(j) == -1 ? fix_lo : 0);
+          if (j < 18 && ((bc0 >> oj) & 1u)) a = (long long)oj * g.plane + i0;
+          st_fast<SP>(A + a, p0[j], j, rho0);
+        }
+        if (!solid1) {
+          long long a = i0 + 1 + o - (cx(j) == 1 ? fix_hi : 0);
+          if (j < 18 && ((bc1 >> oj) & 1u)) a = (long long)oj * g.plane + i0 + 1;
+          st_fast<SP>(A + a, p1[j], j, rho0);
+        }
+      }
+      if (p.compute_force && (bc0 | bc1)) {
+        pair_links<SP>(p, x0, y, z, bc0, p0, acc);
+        pair_links<SP>(p, x0 + 1, y, z, bc1, p1, acc);
+        has_link = true;
+      }
+    }
+  } else {
+    if (inb && !solid0) aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x0, y, z, i0, (uint8_t)fl0, acc, &has_link);
+    if (inb && !solid1) aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x0 + 1, y, z, i0 + 1, (uint8_t)fl1, acc, &has_link);
+  }
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
+}
+
 // q = n / d and r = n % d for n < 2^31 through an FP64 reciprocal (exact after the
 // one-step correction; the product is off by at most one).
 __device__ __forceinline__ void divmod_rcp(const unsigned n, const int d, const double inv, unsigned& q, int& r) {
@@ -1049,6 +1236,13 @@ __global__ void aa_init_kernel(const InitParams p, typename SP::S* __restrict__ 
 template <class SP, bool ODD, bool TRT, bool FORCE, bool FACES>
 static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, dim3 grid, dim3 block,
                               cudaStream_t s) {
+  if constexpr (!FACES) {
+    if (p.pair) {  // 64 x 4 threads, two cells each
+      const dim3 pb(64, 4, 1), pg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 3) / 4), (unsigned)p.g.nz);
+      aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+      return cudaGetLastError();
+    }
+  }
   if (p.tma.enabled) {
     auto kern = aa_tma_kernel<SP, ODD, TRT, FORCE>;
     const int smem = p.tma.stages * p.tma.stage_bytes;

@@ -38,6 +38,7 @@ struct AAParams {
   // per-node link words of NEAR nodes (see near_kernel): static no-slip links stay
   // on the fast path, everything else takes the general path
   const unsigned long long* links;
+  int pair;  // all axes periodic, nx % 128 == 0: two cells per thread (aa_pair_kernel)
 };
 
 // Batched step over many independent config-mode domains (one launch per step).
