@@ -4,7 +4,8 @@
 Workload (the roofline configuration): 512^3 D3Q19, BGK tau=0.6, fully periodic,
 uniform body force g_x=1e-6 (Guo), porous solid of 200 overlapping spheres
 (radius U[6,16], centres U[0,512)^3, numpy default_rng(3)), initial rho=1, u=0,
-FP32 populations.  One step = one fused AA-pattern kernel launch over all cells.
+FP32 populations.  One step = one fused AA-pattern kernel launch over all cells (two x-adjacent
+cells per thread for FP32 and FP16-deviation storage on this box).
 MLUPS counts every cell, solid included (the reference's measure_Mlups,
 Utilities.jl:903-926).
 
@@ -66,9 +67,20 @@ def load_peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
+def step_kernel(storage: str, n: int) -> str:
+    """The kernel a fully periodic n^3 box runs (two cells per thread for FP32 and
+    FP16-deviation when n is a multiple of 128)."""
+    pair = n % 128 == 0 and storage != "fp64"
+    env = os.environ.get("LBM3D_PAIR")
+    if env is not None:
+        pair = n % 128 == 0 and env == "1"
+    return "aa_pair_kernel" if pair else "aa_step_kernel"
+
+
 def profiled_traffic(storage: str, n: int):
     """DRAM bytes per cell of the step kernel from the committed ncu summary."""
-    f = ROOT / "profiles" / f"aa_step_{storage}_porous.txt"
+    kind = "pair" if step_kernel(storage, n) == "aa_pair_kernel" else "step"
+    f = ROOT / "profiles" / f"aa_{kind}_{storage}_porous.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -258,7 +270,9 @@ def run_reference_arm(args, rank: int, world: int):
 def roofline(storage, ms_per_launch, n_cells, n_solid, peak, peak_kind, traffic):
     bytes_launch = (n_cells - n_solid) * BYTES_PER_CELL[storage] + n_solid * 1
     achieved = bytes_launch / (ms_per_launch * 1e-3) / 1e9
-    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+    n = round(n_cells ** (1.0 / 3.0))
+    return {"kernel": step_kernel(storage, n), "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
             "traffic": None if traffic is None else round(traffic, 0),
             "algorithmic_bytes_per_launch": bytes_launch}
