@@ -700,6 +700,9 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);
   if (c->cuda(cudaMemset(c->ring, 0, ring_bytes), "memset ring")) return bail(LBM_ERR_CUDA);
   if (c->A && c->cuda(cudaMemset(c->A, 0, pop), "memset populations")) return bail(LBM_ERR_CUDA);
+  // the clears above run on the legacy stream, which does not order with a non-blocking
+  // stream given later (lbm_set_stream): finish them before any kernel can follow
+  if (c->cuda(cudaStreamSynchronize(cudaStreamLegacy), "clear")) return bail(LBM_ERR_CUDA);
   *out = c;
   return LBM_OK;
 }
@@ -1351,12 +1354,18 @@ int32_t lbm_batch_create(lbm_ctx* const* ctxs, int32_t count, lbm_batch** out) {
   if (b->cuda(cudaMalloc(&b->d_doms, (size_t)count * sizeof(BatchDom)), "cudaMalloc(batch table)")) return bail(LBM_ERR_CUDA);
   if (b->cuda(cudaMalloc(&b->d_item_dom, (size_t)items * sizeof(int)), "cudaMalloc(item map)")) return bail(LBM_ERR_CUDA);
   if (b->cuda(cudaMalloc(&b->d_counter, sizeof(long long)), "cudaMalloc(counter)")) return bail(LBM_ERR_CUDA);
-  if (b->cuda(cudaMemcpy(b->d_doms, b->host.data(), (size_t)count * sizeof(BatchDom), cudaMemcpyHostToDevice), "H2D"))
+  // on the members' stream (it may be non-blocking, so legacy-stream copies would not
+  // order with the batch's kernels); the synchronisation below also ends the members'
+  // earlier work (initialisation, single steps) before the batch
+  if (b->cuda(cudaMemcpyAsync(b->d_doms, b->host.data(), (size_t)count * sizeof(BatchDom), cudaMemcpyHostToDevice,
+                              b->stream),
+              "H2D"))
     return bail(LBM_ERR_CUDA);
-  if (b->cuda(cudaMemcpy(b->d_item_dom, item_dom.data(), (size_t)items * sizeof(int), cudaMemcpyHostToDevice), "H2D"))
+  if (b->cuda(cudaMemcpyAsync(b->d_item_dom, item_dom.data(), (size_t)items * sizeof(int), cudaMemcpyHostToDevice,
+                              b->stream),
+              "H2D"))
     return bail(LBM_ERR_CUDA);
-  if (b->cuda(cudaMemset(b->d_counter, 0, sizeof(long long)), "memset")) return bail(LBM_ERR_CUDA);
-  // members' earlier work (initialisation, single steps) precedes the batch
+  if (b->cuda(cudaMemsetAsync(b->d_counter, 0, sizeof(long long), b->stream), "memset")) return bail(LBM_ERR_CUDA);
   if (b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize")) return bail(LBM_ERR_CUDA);
   *out = b;
   return LBM_OK;
