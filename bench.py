@@ -69,17 +69,20 @@ def load_peaks() -> tuple[float, str]:
 
 def step_kernel(storage: str, n: int) -> str:
     """The kernel a fully periodic n^3 box runs (two cells per thread for FP32 and
-    FP16-deviation when n is a multiple of 128)."""
+    FP16-deviation when n is a multiple of 128; FP16-deviation odd steps run the split
+    variant)."""
     pair = n % 128 == 0 and storage != "fp64"
     env = os.environ.get("LBM3D_PAIR")
     if env is not None:
         pair = n % 128 == 0 and env == "1"
-    return "aa_pair_kernel" if pair else "aa_step_kernel"
+    if not pair:
+        return "aa_step_kernel"
+    return "aa_pair_kernel / aa_pair_split_kernel" if storage == "fp16dev" else "aa_pair_kernel"
 
 
 def profiled_traffic(storage: str, n: int):
     """DRAM bytes per cell of the step kernel from the committed ncu summary."""
-    kind = "pair" if step_kernel(storage, n) == "aa_pair_kernel" else "step"
+    kind = "pair" if step_kernel(storage, n).startswith("aa_pair_kernel") else "step"
     f = ROOT / "profiles" / f"aa_{kind}_{storage}_porous.txt"
     if not f.exists():
         return None

@@ -852,6 +852,146 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_ker
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
+// Odd-phase variant of the pair kernel (FP16-deviation storage): a cell's odd-phase
+// writes are read back only by the same cell in the next step, so cell 0 stores its
+// x-shifted outputs before cell 1 collides and only the nine values that pair with
+// cell 1 stay live.  Row bases with the periodic x wrap folded in keep the addressing
+// to one add per access.  Measured on B200 (512^3 porous box): 11 % faster than the
+// joint pair kernel for FP16 storage; slower for FP32 and for the even phase, which
+// keep aa_pair_kernel.
+template <class SP, bool TRT, bool FORCE>
+__global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_split_kernel(const __grid_constant__ AAParams p,
+                                                                                typename SP::S* __restrict__ A,
+                                                                                const uint8_t* __restrict__ flags) {
+  using S = typename SP::S;
+  using C = typename SP::C;
+  const Grid& g = p.g;
+  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = x0 < g.nx && y < g.ny;
+  clear_record(p.zero_next);
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  const long long i0 = inb ? node_index(g, x0, y, z) : 0;
+  const bool coord_fast = inb && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
+  uint32_t fl0 = F_SOLID, fl1 = F_SOLID;
+  if (inb) {
+    const uint32_t fw = *reinterpret_cast<const unsigned short*>(flags + i0);
+    fl0 = fw & 0xFFu;
+    fl1 = fw >> 8;
+  }
+  // Row bases with the periodic x wrap folded in: cell 0 at x = 0 reaches x = -1 at
+  // x = nx - 1 (pull with c_x = +1, push with c_x = -1), cell 1 at x = nx - 1 reaches
+  // x = nx at x = 0 (pull with c_x = -1, push with c_x = +1).
+  S* const Ai = A + i0;
+  S* const A0 = Ai + (x0 == 0 ? (long long)g.nx : 0);
+  S* const A1 = Ai + 1 - (x0 + 1 == g.nx - 1 ? (long long)g.nx : 0);
+  C f0[Q], f1[Q];
+  if (coord_fast) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      const long long o = p.off_rd[d];
+      if (cx(d) == 0) {
+        Pair2<S>::ld(Ai + o, f0[d], f1[d]);
+      } else if (cx(d) == 1) {
+        f0[d] = ld_fast<SP>(A0 + o, d, C(p.rho0));
+        f1[d] = ld_fast<SP>(Ai + o + 1, d, C(p.rho0));
+      } else {
+        f0[d] = ld_fast<SP>(Ai + o, d, C(p.rho0));
+        f1[d] = ld_fast<SP>(A1 + o, d, C(p.rho0));
+      }
+    }
+  }
+  const bool solid0 = (fl0 & F_SOLID) != 0, solid1 = (fl1 & F_SOLID) != 0;
+  uint32_t bc0 = 0, bc1 = 0;
+  bool st0 = true, st1 = true;
+  if (!solid0 && (fl0 & F_NEAR)) {
+    const unsigned long long lw = p.links[i0];
+    bc0 = (uint32_t)(lw & 0x3FFFFu);
+    st0 = bc0 == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 && !(fl0 & F_SOLID_PREV);
+  }
+  if (!solid1 && (fl1 & F_NEAR)) {
+    const unsigned long long lw = p.links[i0 + 1];
+    bc1 = (uint32_t)(lw & 0x3FFFFu);
+    st1 = bc1 == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 && !(fl1 & F_SOLID_PREV);
+  }
+  const bool both_solid = solid0 && solid1;
+  const bool fast = coord_fast && st0 && st1;
+  if (__all_sync(0xffffffffu, both_solid || fast)) {
+    if (!both_solid) {
+      if (bc0 | bc1) {  // bounce-back values are kept in the own slots
+#pragma unroll
+        for (int d = 0; d < 18; d++) {
+          if ((bc0 >> d) & 1u) f0[d] = ld_fast<SP>(Ai + (long long)d * g.plane, d, C(p.rho0));
+          if ((bc1 >> d) & 1u) f1[d] = ld_fast<SP>(Ai + 1 + (long long)d * g.plane, d, C(p.rho0));
+        }
+      }
+      const bool plain = !solid0 && !solid1 && !(bc0 | bc1);
+      const C rho0 = C(p.rho0);
+      C p0[Q];
+      if (!solid0) {
+        pair_cell<SP, true, TRT, FORCE>(p, f0, p0);
+      } else {
+#pragma unroll
+        for (int d = 0; d < Q; d++) p0[d] = C(0);
+      }
+      if (plain) {  // x-shifted directions of cell 0 (the others pair below)
+#pragma unroll
+        for (int j = 0; j < Q; j++)
+          if (cx(j) != 0) st_fast<SP>((cx(j) == 1 ? Ai : A0) + p.off_wr[j], p0[j], j, rho0);
+      } else if (!solid0) {
+#pragma unroll
+        for (int j = 0; j < Q; j++) {
+          const int oj = opp(j);
+          S* a = (cx(j) == -1 ? A0 : Ai) + p.off_wr[j];
+          if (j < 18 && ((bc0 >> oj) & 1u)) a = Ai + (long long)oj * g.plane;
+          st_fast<SP>(a, p0[j], j, rho0);
+        }
+      }
+      if (p.compute_force && bc0) {
+        pair_links<SP>(p, x0, y, z, bc0, p0, acc);
+        has_link = true;
+      }
+      C p1[Q];
+      if (!solid1) {
+        pair_cell<SP, true, TRT, FORCE>(p, f1, p1);
+      } else {
+#pragma unroll
+        for (int d = 0; d < Q; d++) p1[d] = C(0);
+      }
+      if (plain) {
+#pragma unroll
+        for (int j = 0; j < Q; j++) {
+          const long long o = p.off_wr[j];
+          if (cx(j) == 0)
+            Pair2<S>::st(Ai + o, p0[j], p1[j]);
+          else
+            st_fast<SP>(cx(j) == 1 ? A1 + o : Ai + o + 1, p1[j], j, rho0);
+        }
+      } else if (!solid1) {
+#pragma unroll
+        for (int j = 0; j < Q; j++) {
+          const int oj = opp(j);
+          const long long o = p.off_wr[j];
+          S* a = cx(j) == 1 ? A1 + o : Ai + o + 1;
+          if (j < 18 && ((bc1 >> oj) & 1u)) a = Ai + 1 + (long long)oj * g.plane;
+          st_fast<SP>(a, p1[j], j, rho0);
+        }
+      }
+      if (p.compute_force && bc1) {
+        pair_links<SP>(p, x0 + 1, y, z, bc1, p1, acc);
+        has_link = true;
+      }
+    }
+  } else {
+    if (inb && !solid0) aa_general<SP, true, TRT, FORCE>(p, A, flags, x0, y, z, i0, (uint8_t)fl0, acc, &has_link);
+    if (inb && !solid1) aa_general<SP, true, TRT, FORCE>(p, A, flags, x0 + 1, y, z, i0 + 1, (uint8_t)fl1, acc, &has_link);
+  }
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
+}
+
+
 // q = n / d and r = n % d for n < 2^31 through an FP64 reciprocal (exact after the
 // one-step correction; the product is off by at most one).
 __device__ __forceinline__ void divmod_rcp(const unsigned n, const int d, const double inv, unsigned& q, int& r) {
@@ -1239,7 +1379,10 @@ static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, 
   if constexpr (!FACES) {
     if (p.pair) {  // 64 x 4 threads, two cells each
       const dim3 pb(64, 4, 1), pg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 3) / 4), (unsigned)p.g.nz);
-      aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+      if constexpr (ODD && SP::DEV)
+        aa_pair_split_kernel<SP, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+      else
+        aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
       return cudaGetLastError();
     }
   }
