@@ -179,11 +179,18 @@ __device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rh
     const C om = k.om_p, omc = C(1) - k.om_p;
     // omega * e = B + T (c.u)^2 ; omega * o = O (c.u)
     const C rb = rho * base - rho0;  // DEV only
-    const C B1 = DEV ? om * wgt<C>(0) * rb : om * wr1 * base, B2 = DEV ? om * wgt<C>(6) * rb : om * wr2 * base;
+    C B1 = DEV ? om * wgt<C>(0) * rb : om * wr1 * base, B2 = DEV ? om * wgt<C>(6) * rb : om * wr2 * base;
     const C T1 = C(4.5) * om * wr1, T2 = C(4.5) * om * wr2;
     const C O1 = C(3) * om * wr1, O2 = C(3) * om * wr2;
     const C fac = C(1) - C(0.5) * om;
     const C G1 = fac * wgt<C>(0), G2 = fac * wgt<C>(6);
+    // FP16 deviations: the direction-independent source part w (-3 u.F) joins the
+    // constant of e (one FMA less per direction pair; measured faster on B200 for the
+    // issue-bound FP16 kernels, slower for FP32, which keeps the unfolded form)
+    if (FORCE && DEV) {
+      B1 += G1 * m3uF;
+      B2 += G2 * m3uF;
+    }
 #pragma unroll
     for (int q = 0; q < 9; q++) {
       const int d = 2 * q;
@@ -194,7 +201,10 @@ __device__ __forceinline__ void collide(const C* f, C* p, const Coll<C>& k, C rh
       if (FORCE) {
         const C cF = cdot<C>(d, Fx, Fy, Fz);
         const C G = c1 ? G1 : G2;
-        e += G * (C(9) * (cu * cF) + m3uF);
+        if (DEV)
+          e += (C(9) * G) * (cu * cF);
+        else
+          e += G * (C(9) * (cu * cF) + m3uF);
         o += (C(3) * G) * cF;
       }
       p[d] = omc * f[d] + (e + o);
@@ -887,19 +897,22 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_spl
   S* const Ai = A + i0;
   S* const A0 = Ai + (x0 == 0 ? (long long)g.nx : 0);
   S* const A1 = Ai + 1 - (x0 + 1 == g.nx - 1 ? (long long)g.nx : 0);
+  // read / write / own slot of direction d relative to a row base
+  const auto rd = [&](S* b, int d) { return b + p.off_rd[d]; };
+  const auto wr = [&](S* b, int d) { return b + p.off_wr[d]; };
+  const auto own = [&](S* b, int d) { return b + (long long)d * g.plane; };
   C f0[Q], f1[Q];
   if (coord_fast) {
 #pragma unroll
     for (int d = 0; d < Q; d++) {
-      const long long o = p.off_rd[d];
       if (cx(d) == 0) {
-        Pair2<S>::ld(Ai + o, f0[d], f1[d]);
+        Pair2<S>::ld(rd(Ai, d), f0[d], f1[d]);
       } else if (cx(d) == 1) {
-        f0[d] = ld_fast<SP>(A0 + o, d, C(p.rho0));
-        f1[d] = ld_fast<SP>(Ai + o + 1, d, C(p.rho0));
+        f0[d] = ld_fast<SP>(rd(A0, d), d, C(p.rho0));
+        f1[d] = ld_fast<SP>(rd(Ai, d) + 1, d, C(p.rho0));
       } else {
-        f0[d] = ld_fast<SP>(Ai + o, d, C(p.rho0));
-        f1[d] = ld_fast<SP>(A1 + o, d, C(p.rho0));
+        f0[d] = ld_fast<SP>(rd(Ai, d), d, C(p.rho0));
+        f1[d] = ld_fast<SP>(rd(A1, d), d, C(p.rho0));
       }
     }
   }
@@ -923,8 +936,8 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_spl
       if (bc0 | bc1) {  // bounce-back values are kept in the own slots
 #pragma unroll
         for (int d = 0; d < 18; d++) {
-          if ((bc0 >> d) & 1u) f0[d] = ld_fast<SP>(Ai + (long long)d * g.plane, d, C(p.rho0));
-          if ((bc1 >> d) & 1u) f1[d] = ld_fast<SP>(Ai + 1 + (long long)d * g.plane, d, C(p.rho0));
+          if ((bc0 >> d) & 1u) f0[d] = ld_fast<SP>(own(Ai, d), d, C(p.rho0));
+          if ((bc1 >> d) & 1u) f1[d] = ld_fast<SP>(own(Ai, d) + 1, d, C(p.rho0));
         }
       }
       const bool plain = !solid0 && !solid1 && !(bc0 | bc1);
@@ -939,13 +952,13 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_spl
       if (plain) {  // x-shifted directions of cell 0 (the others pair below)
 #pragma unroll
         for (int j = 0; j < Q; j++)
-          if (cx(j) != 0) st_fast<SP>((cx(j) == 1 ? Ai : A0) + p.off_wr[j], p0[j], j, rho0);
+          if (cx(j) != 0) st_fast<SP>(wr(cx(j) == 1 ? Ai : A0, j), p0[j], j, rho0);
       } else if (!solid0) {
 #pragma unroll
         for (int j = 0; j < Q; j++) {
           const int oj = opp(j);
-          S* a = (cx(j) == -1 ? A0 : Ai) + p.off_wr[j];
-          if (j < 18 && ((bc0 >> oj) & 1u)) a = Ai + (long long)oj * g.plane;
+          S* a = wr(cx(j) == -1 ? A0 : Ai, j);
+          if (j < 18 && ((bc0 >> oj) & 1u)) a = own(Ai, oj);
           st_fast<SP>(a, p0[j], j, rho0);
         }
       }
@@ -963,19 +976,17 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_spl
       if (plain) {
 #pragma unroll
         for (int j = 0; j < Q; j++) {
-          const long long o = p.off_wr[j];
           if (cx(j) == 0)
-            Pair2<S>::st(Ai + o, p0[j], p1[j]);
+            Pair2<S>::st(wr(Ai, j), p0[j], p1[j]);
           else
-            st_fast<SP>(cx(j) == 1 ? A1 + o : Ai + o + 1, p1[j], j, rho0);
+            st_fast<SP>(cx(j) == 1 ? wr(A1, j) : wr(Ai, j) + 1, p1[j], j, rho0);
         }
       } else if (!solid1) {
 #pragma unroll
         for (int j = 0; j < Q; j++) {
           const int oj = opp(j);
-          const long long o = p.off_wr[j];
-          S* a = cx(j) == 1 ? A1 + o : Ai + o + 1;
-          if (j < 18 && ((bc1 >> oj) & 1u)) a = Ai + 1 + (long long)oj * g.plane;
+          S* a = cx(j) == 1 ? wr(A1, j) : wr(Ai, j) + 1;
+          if (j < 18 && ((bc1 >> oj) & 1u)) a = own(Ai, oj) + 1;
           st_fast<SP>(a, p1[j], j, rho0);
         }
       }
