@@ -63,9 +63,12 @@ enum {
   LBM_FACE_WALL = 1,     /* half-way bounce-back, wall velocity face_u[f] (0: no-slip) */
   LBM_FACE_EQ_INLET = 2, /* unknown populations set to feq(rho_node, face_u[f]) */
   LBM_FACE_OUTFLOW = 3,  /* zero-gradient: unknown population = same node's post-collision value */
-  LBM_FACE_PRESSURE = 4  /* pressure outlet: anti-bounce-back at rho0 with the node's velocity
+  LBM_FACE_PRESSURE = 4, /* pressure outlet: anti-bounce-back at rho0 with the node's velocity
                             (the outlet rule of velocity_BC!_gpu, OtherBC.jl:153-166, with the
                             density fixed to rho0 instead of the node's) */
+  LBM_FACE_HALO = 5      /* z faces only: the plane on this face is a ghost plane of a z-slab
+                            decomposition (lbm_halo_pack / lbm_halo_unpack); it is never updated,
+                            and its nodes are ordinary fluid or solid neighbours of the slab */
 };
 
 /* Body kinds. CYLINDER_Z and NACA_Z are the reference's extruded shapes
@@ -303,6 +306,29 @@ int32_t lbm_batch_replay(lbm_batch* b, int32_t times);
 int64_t lbm_batch_launch_count(const lbm_batch* b);
 /* Waits for the members' stream; LBM_ERR_CUDA with the CUDA error otherwise. */
 int32_t lbm_batch_synchronize(lbm_batch* b);
+
+/* ---- z-slab decomposition (replaces the halo exchange of Exchange.jl) ----
+ * A domain split along z into slabs, one context per slab (per GPU), each holding its
+ * owned planes plus one ghost plane on every LBM_FACE_HALO face (z = 0 and/or
+ * z = nz - 1 of the slab).  Static bodies only (bodies placed in slab coordinates, the
+ * ghost planes included).  After EVERY step, on each halo face, the caller moves one
+ * message from this slab to the neighbouring slab and one back:
+ *     lbm_halo_pack(mine, side, buf)  ->  transport  ->  lbm_halo_unpack(neighbour, 1 - side, buf)
+ * The message of a face is 5 populations (the directions crossing it) times nx*ny
+ * elements of the storage type: lbm_halo_bytes().  After an even-phase step the
+ * boundary plane's post-collision values fill the neighbour's ghost plane; after an
+ * odd-phase step the values streamed into the ghost plane go to the neighbour's
+ * boundary plane (where the ghost node is fluid; a bounce-back value the neighbour
+ * wrote itself is kept).  The phase follows from the context's step count, so both
+ * calls must come after the same step on both sides.  Enqueued on the context's stream.
+ * Replaces begin_halo_exchange! / gather_halo! (Exchange.jl:11-66, 112-129) and
+ * finish_halo_exchange! / scatter_halo! (Exchange.jl:69-107, 131-145); the
+ * transport between the calls (MPI Isend/Irecv there) is the caller's. */
+int64_t lbm_halo_bytes(const lbm_ctx* ctx);
+/* side: 0 = z-lo face, 1 = z-hi face (must be LBM_FACE_HALO).  d_buf: device memory of
+ * lbm_halo_bytes() bytes. */
+int32_t lbm_halo_pack(lbm_ctx* ctx, int32_t side, void* d_buf);
+int32_t lbm_halo_unpack(lbm_ctx* ctx, int32_t side, const void* d_buf);
 
 #ifdef __cplusplus
 }

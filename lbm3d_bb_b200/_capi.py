@@ -63,6 +63,9 @@ def lib() -> C.CDLL:
         "lbm_get_flags": (i32, [vp, vp, vp]),
         "lbm_get_links": (i32, [vp, vp, vp, vp, i64, P(i64)]),
         "lbm_get_links_noalloc": (i32, [vp, vp, vp, vp, i64, P(i64)]),
+        "lbm_halo_bytes": (i64, [vp]),
+        "lbm_halo_pack": (i32, [vp, i32, vp]),
+        "lbm_halo_unpack": (i32, [vp, i32, vp]),
         "lbm_mass": (i32, [vp, P(f64)]),
         "lbm_check": (i32, [vp]),
         "lbm_batch_create": (i32, [vp, i32, P(vp)]),
@@ -95,6 +98,7 @@ def exported_symbols() -> list[str]:
         "lbm_get_links", "lbm_get_links_noalloc", "lbm_mass", "lbm_check",
         "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_last_error", "lbm_batch_step", "lbm_batch_capture",
         "lbm_batch_replay", "lbm_batch_launch_count", "lbm_batch_synchronize",
+        "lbm_halo_bytes", "lbm_halo_pack", "lbm_halo_unpack",
     ]
 
 

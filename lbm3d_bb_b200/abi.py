@@ -31,6 +31,7 @@ FACE_WALL = 1
 FACE_EQ_INLET = 2
 FACE_OUTFLOW = 3
 FACE_PRESSURE = 4
+FACE_HALO = 5
 
 BODY_CYLINDER_Z = 1
 BODY_NACA_Z = 2
@@ -47,7 +48,7 @@ DEVICE = 1
 STORAGE = {"fp32": STORE_FP32, "fp64": STORE_FP64, "fp16dev": STORE_FP16DEV}
 COLLISION = {"BGK": COLL_BGK, "TRT": COLL_TRT}
 FACES = {"periodic": FACE_PERIODIC, "wall": FACE_WALL, "inlet": FACE_EQ_INLET, "outflow": FACE_OUTFLOW,
-         "pressure": FACE_PRESSURE}
+         "pressure": FACE_PRESSURE, "halo": FACE_HALO}
 
 
 class LbmConfig(C.Structure):

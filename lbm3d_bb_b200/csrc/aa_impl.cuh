@@ -638,7 +638,11 @@ __device__ __forceinline__ void aa_direct(const AAParams& p, typename SP::S* __r
   const uint8_t fl = inb ? flags[i] : (uint8_t)F_SOLID;
   C f[Q];
   if (coord_fast) aa_fast_load<SP, ODD, FACES>(p, A + i, x, fc.mask, f);
-  const bool solid = (fl & F_SOLID) != 0;
+  // the ghost plane on a halo face (z-slab decomposition) is read and written by its
+  // neighbours like any fluid or solid node but never updated itself
+  const bool ghost = FACES && inb &&
+                     ((z == 0 && p.face_kind[4] == LBM_FACE_HALO) || (z == g.nz - 1 && p.face_kind[5] == LBM_FACE_HALO));
+  const bool solid = (fl & F_SOLID) != 0 || ghost;
   // fast when the only boundaries are static no-slip links (link word: current ==
   // previous links, no moving-body link, not uncovered)
   uint32_t bc = 0;

@@ -402,6 +402,9 @@ void fill_aa_params(const lbm_ctx* c, AAParams& p, bool odd) {
 
 bool has_force(const lbm_ctx* c) { return c->cfg.accel[0] != 0.0 || c->cfg.accel[1] != 0.0 || c->cfg.accel[2] != 0.0; }
 bool has_faces(const lbm_ctx* c) { return !(c->g.per[0] && c->g.per[1] && c->g.per[2]); }
+bool has_halo(const lbm_ctx* c) {
+  return !c->ref && (c->cfg.face[4] == LBM_FACE_HALO || c->cfg.face[5] == LBM_FACE_HALO);
+}
 
 int near_full(lbm_ctx* c) {
   c->tiles_dirty = true;
@@ -612,10 +615,14 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     for (int a = 0; a < 3; a++) {
       const bool p0 = cfg->face[2 * a] == LBM_FACE_PERIODIC, p1 = cfg->face[2 * a + 1] == LBM_FACE_PERIODIC;
       if (p0 != p1) return set_global(LBM_ERR_ARG, "axis %d: both faces periodic or neither", a);
-      for (int s = 0; s < 2; s++)
-        if (cfg->face[2 * a + s] < LBM_FACE_PERIODIC || cfg->face[2 * a + s] > LBM_FACE_PRESSURE)
+      for (int s = 0; s < 2; s++) {
+        if (cfg->face[2 * a + s] < LBM_FACE_PERIODIC || cfg->face[2 * a + s] > LBM_FACE_HALO)
           return set_global(LBM_ERR_ARG, "bad face kind");
+        if (cfg->face[2 * a + s] == LBM_FACE_HALO && a != 2) return set_global(LBM_ERR_ARG, "halo faces are z faces");
+      }
     }
+    if ((cfg->face[4] == LBM_FACE_HALO || cfg->face[5] == LBM_FACE_HALO) && cfg->nz < 3)
+      return set_global(LBM_ERR_ARG, "a slab with halo faces needs nz >= 3");
   }
   lbm_ctx* c = new lbm_ctx();
   c->cfg = *cfg;
@@ -676,7 +683,8 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
   {
     const char* on = std::getenv("LBM3D_TMA");
     const int tw = 128;
-    if (!c->ref && (on && on[0] == '1') && cfg->nx % tw == 0 && (cfg->nx * (long long)c->elem) % 16 == 0) {
+    if (!c->ref && (on && on[0] == '1') && cfg->nx % tw == 0 && (cfg->nx * (long long)c->elem) % 16 == 0 &&
+        !has_halo(c)) {
       c->tma = true;
       c->tma_tw = tw;
       c->ntiles = c->g.N / tw;
@@ -778,6 +786,7 @@ int32_t lbm_add_body(lbm_ctx* c, const lbm_body* b) {
   }
   if (b->moving) {
     if (c->has_moving) return c->fail(LBM_ERR_ARG, "at most one moving body");
+    if (has_halo(c)) return c->fail(LBM_ERR_UNSUPPORTED, "slabs with halo faces take static bodies only");
     c->has_moving = true;
     c->moving_body = *b;
     lbm_pose p0{};
@@ -1450,5 +1459,27 @@ int32_t lbm_batch_synchronize(lbm_batch* b) {
   if (b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) return LBM_ERR_CUDA;
   return b->cuda(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
 }
+
+// ---- z-slab halo messages ----
+int64_t lbm_halo_bytes(const lbm_ctx* c) {
+  if (!c || !has_halo(c)) return 0;
+  return 5LL * c->g.nx * c->g.ny * c->elem;
+}
+
+static int32_t halo_call(lbm_ctx* c, int32_t side, const void* buf, bool pack) {
+  if (!c || !buf) return LBM_ERR_ARG;
+  if (side != 0 && side != 1) return c->fail(LBM_ERR_ARG, "side must be 0 (z-lo) or 1 (z-hi)");
+  if (c->ref || c->cfg.face[4 + side] != LBM_FACE_HALO)
+    return c->fail(LBM_ERR_ARG, "face %d is not a halo face", 4 + side);
+  if (!c->initialised) return c->fail(LBM_ERR_STATE, "initialise the populations first");
+  if (c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  // swapped layout <=> the last step was an even-phase step
+  return c->cuda(aa_launch_halo(c->g, c->elem, side, c->swapped, pack, c->A, c->flags, const_cast<void*>(buf),
+                                c->stream),
+                 pack ? "halo pack" : "halo unpack");
+}
+
+int32_t lbm_halo_pack(lbm_ctx* c, int32_t side, void* d_buf) { return halo_call(c, side, d_buf, true); }
+int32_t lbm_halo_unpack(lbm_ctx* c, int32_t side, const void* d_buf) { return halo_call(c, side, d_buf, false); }
 
 }  // extern "C"

@@ -117,4 +117,73 @@ cudaError_t aa_launch_batch_advance(long long* counter, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// ---- z-slab halo messages ------------------------------------------------------------
+// One thread per (crossing direction k, x, y) of a face.  `inward` = c_z of the
+// directions entering the slab through this face (+1 at z-lo, -1 at z-hi).
+//   after an even-phase step (swapped layout):
+//     pack   the boundary plane's slots with c_z = inward (post-collision values that the
+//            neighbour's first plane pulls across the face in the odd phase);
+//     unpack into the ghost plane's slots with c_z = -inward (the neighbour's values that
+//            this slab's boundary plane pulls);
+//   after an odd-phase step:
+//     pack   the ghost plane's slots with c_z = -inward (what the boundary plane pushed
+//            across the face: they belong to the neighbour's boundary plane);
+//     unpack into the boundary plane's slots with c_z = inward, only where the source node
+//            x - c_d (a ghost node) is fluid: otherwise the node wrote that slot itself
+//            (bounce-back) or, outside a non-periodic face, its face rule did.
+// The crossing directions are taken in ascending order on both sides of a face, so a
+// message packed by one slab unpacks unchanged in its neighbour.
+template <class T>
+__global__ void halo_kernel(const Grid g, const int side, const int after_even, const int pack, T* __restrict__ A,
+                            const uint8_t* __restrict__ flags, T* __restrict__ buf) {
+  const long long nxy = (long long)g.nx * g.ny;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 5 * nxy) return;
+  const int k = (int)(t / nxy);
+  const long long r = t - (long long)k * nxy;
+  const int y = (int)(r / g.nx), x = (int)(r - (long long)y * g.nx);
+  const int inward = side == 0 ? 1 : -1;
+  const int zg = side == 0 ? 0 : g.nz - 1;  // ghost plane
+  const int zb = zg + inward;                // boundary plane
+  // slot set and plane of this call
+  const bool boundary_side = after_even ? pack : !pack;
+  const int sgn = boundary_side ? inward : -inward;
+  const int z = boundary_side ? zb : zg;
+  int d = -1;
+  for (int e = 0, n = 0; e < 19; e++)
+    if (cz(e) == sgn && n++ == k) d = e;
+  T* slot = A + (long long)d * g.plane + node_index(g, x, y, z);
+  if (pack) {
+    buf[t] = *slot;
+    return;
+  }
+  if (!after_even) {
+    int sx = x - cx(d), sy = y - cy(d);
+    if (sx < 0 || sx >= g.nx) {
+      if (!g.per[0]) return;
+      sx = (sx + g.nx) % g.nx;
+    }
+    if (sy < 0 || sy >= g.ny) {
+      if (!g.per[1]) return;
+      sy = (sy + g.ny) % g.ny;
+    }
+    if (flags[node_index(g, sx, sy, zg)] & F_SOLID) return;
+  }
+  *slot = buf[t];
+}
+
+cudaError_t aa_launch_halo(const Grid& g, int elem, int side, bool after_even, bool pack, void* A,
+                           const uint8_t* flags, void* buf, cudaStream_t s) {
+  const long long n = 5LL * g.nx * g.ny;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  const int ae = after_even ? 1 : 0, pk = pack ? 1 : 0;
+  if (elem == 2)
+    halo_kernel<uint16_t><<<blocks, 256, 0, s>>>(g, side, ae, pk, (uint16_t*)A, flags, (uint16_t*)buf);
+  else if (elem == 4)
+    halo_kernel<uint32_t><<<blocks, 256, 0, s>>>(g, side, ae, pk, (uint32_t*)A, flags, (uint32_t*)buf);
+  else
+    halo_kernel<uint64_t><<<blocks, 256, 0, s>>>(g, side, ae, pk, (uint64_t*)A, flags, (uint64_t*)buf);
+  return cudaGetLastError();
+}
+
 }  // namespace lbm

@@ -209,6 +209,9 @@ cudaError_t aa_launch_batch(int storage, const BatchParams& bp, bool trt, bool f
                             cudaStream_t s);
 cudaError_t aa_batch_blocks_per_sm(int storage, bool trt, bool force, bool faces, int* per_sm);
 cudaError_t aa_launch_batch_advance(long long* counter, cudaStream_t s);
+// z-slab halo message of one face (side 0 z-lo, 1 z-hi); elem = bytes per population
+cudaError_t aa_launch_halo(const Grid& g, int elem, int side, bool after_even, bool pack, void* A,
+                           const uint8_t* flags, void* buf, cudaStream_t s);
 cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
                              const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags,

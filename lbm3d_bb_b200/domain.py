@@ -131,6 +131,20 @@ class Domain:
     def step(self, n: int = 1) -> None:
         self._check(self._L.lbm_step(self._h, int(n)))
 
+    # -- z-slab halo messages (faces of kind "halo") -----------------------------------------
+    @property
+    def halo_bytes(self) -> int:
+        """Bytes of one face's message (0 without halo faces)."""
+        return int(self._L.lbm_halo_bytes(self._h))
+
+    def halo_pack(self, side: int, buf) -> None:
+        """Enqueues the message of face `side` (0 z-lo, 1 z-hi) into the device tensor `buf`."""
+        self._check(self._L.lbm_halo_pack(self._h, int(side), _ptr(buf)))
+
+    def halo_unpack(self, side: int, buf) -> None:
+        """Enqueues the merge of the neighbour's message `buf` on face `side`."""
+        self._check(self._L.lbm_halo_unpack(self._h, int(side), _ptr(buf)))
+
     @property
     def step_count(self) -> int:
         return int(self._L.lbm_step_count(self._h))
