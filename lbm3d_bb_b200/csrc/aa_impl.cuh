@@ -604,6 +604,12 @@ __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S
   }
 }
 
+// Ghost plane on a halo face (z-slab decomposition).  The step kernels put one z plane in
+// a block, so a ghost block leaves at once; the batched kernel checks per node.
+__device__ __forceinline__ bool ghost_plane(const AAParams& p, const int z) {
+  return (z == 0 && p.face_kind[4] == LBM_FACE_HALO) || (z == p.g.nz - 1 && p.face_kind[5] == LBM_FACE_HALO);
+}
+
 // One node on the direct path: lanes whose coordinates allow the fast path issue
 // their population loads at once; the flag byte (and, next to a solid, the link
 // word) decides afterwards whether the warp finishes on the fast path or reruns the
@@ -673,6 +679,7 @@ __global__ void __launch_bounds__(256, SP::MIN_BLOCKS) aa_step_kernel(const __gr
   const int z = blockIdx.z;
   const bool inb = (x < g.nx) && (y < g.ny);
   clear_record(p.zero_next);  // the next step's force record (read by the next launch only)
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool has_link = false;
   aa_direct<SP, ODD, TRT, FORCE, FACES>(p, A, flags, x, y, z, inb, acc, &has_link);
@@ -766,6 +773,7 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_ker
   const int z = blockIdx.z;
   const bool inb = x0 < g.nx && y < g.ny;
   clear_record(p.zero_next);
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool has_link = false;
   const long long i0 = inb ? node_index(g, x0, y, z) : 0;
@@ -885,6 +893,7 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_spl
   const int z = blockIdx.z;
   const bool inb = x0 < g.nx && y < g.ny;
   clear_record(p.zero_next);
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool has_link = false;
   const long long i0 = inb ? node_index(g, x0, y, z) : 0;

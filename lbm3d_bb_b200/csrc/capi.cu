@@ -405,6 +405,13 @@ bool has_faces(const lbm_ctx* c) { return !(c->g.per[0] && c->g.per[1] && c->g.p
 bool has_halo(const lbm_ctx* c) {
   return !c->ref && (c->cfg.face[4] == LBM_FACE_HALO || c->cfg.face[5] == LBM_FACE_HALO);
 }
+// periodic x and y, halo faces on both z ends: no face node outside the ghost planes, so
+// the step kernels without face handling (and the pair kernel) serve it, skipping the
+// ghost planes block by block
+bool halo_only(const lbm_ctx* c) {
+  return !c->ref && c->g.per[0] && c->g.per[1] && c->cfg.face[4] == LBM_FACE_HALO &&
+         c->cfg.face[5] == LBM_FACE_HALO;
+}
 
 int near_full(lbm_ctx* c) {
   c->tiles_dirty = true;
@@ -700,7 +707,8 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     // FP32 and FP16-deviation storage (faster on B200: +2 % and +16 % on the 512^3 porous
     // box), not for FP64 (15 % slower); LBM3D_PAIR=1 / 0 forces it on / off
     const char* env = std::getenv("LBM3D_PAIR");
-    const bool fits = !c->ref && !c->tma && cfg->nx % 128 == 0 && c->g.per[0] && c->g.per[1] && c->g.per[2];
+    const bool fits = !c->ref && !c->tma && cfg->nx % 128 == 0 && c->g.per[0] && c->g.per[1] &&
+                      (c->g.per[2] || halo_only(c));
     const bool wanted = env ? env[0] == '1' : cfg->storage != LBM_STORE_FP64;
     c->pair = fits && wanted;
   }
@@ -975,8 +983,8 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
         T.err = c->d_err;
       }
       c->launches++;
-      rc = c->cuda(aa_launch_step(c->cfg.storage, p, c->A, c->flags, c->swapped, trt, has_force(c), has_faces(c),
-                                  c->grid(), c->block(), c->stream),
+      rc = c->cuda(aa_launch_step(c->cfg.storage, p, c->A, c->flags, c->swapped, trt, has_force(c),
+                                  has_faces(c) && !halo_only(c), c->grid(), c->block(), c->stream),
                    "AA step");
       if (rc) return rc;
       c->swapped = !c->swapped;

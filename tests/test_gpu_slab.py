@@ -79,6 +79,36 @@ def test_slabs_reproduce_the_undivided_box(parts, steps, storage, collision, fac
             s.close()
 
 
+@pytest.mark.parametrize("storage,parts,steps", [("fp32", 2, 7), ("fp16dev", 3, 8), ("fp64", 2, 6)])
+def test_slabs_on_the_pair_kernel(storage, parts, steps):
+    """Periodic x and y with nx a multiple of 128: slabs run the pair kernel (FP32 and
+    FP16-deviation) or the one-cell kernel without face handling (FP64), skipping their
+    ghost planes block by block."""
+    nx, ny, nz = 128, 12, 18
+    xyzr = np.array([[20.5, 5.2, 9.1, 3.7], [70.2, 7.7, 0.8, 4.1], [101.3, 3.1, 12.2, 3.3]])
+    kw = _kw(storage, "BGK", cases.PERIODIC)
+    full = Domain(nx, ny, nz, **kw)
+    full.add_spheres(xyzr)
+    full.init_equilibrium()
+    full.step(steps)
+    slabs = [SlabDomain(nx, ny, nz, parts, r, **kw) for r in range(parts)]
+    for s in slabs:
+        s.add_spheres(xyzr)
+        s.init_equilibrium()
+    g = SlabGroup(slabs)
+    g.step(steps)
+    try:
+        f_full = full.populations().reshape(19, nz, ny, nx)
+        f_slab = np.concatenate([s.populations() for s in slabs], axis=1)
+        assert rel_l2(f_slab, f_full) <= TOL[storage]
+        a, b = g.force(steps), full.force(steps)
+        assert np.linalg.norm(a - b) <= 100 * TOL[storage] * np.linalg.norm(b) + 1e-12, (a, b)
+    finally:
+        full.close()
+        for s in slabs:
+            s.close()
+
+
 def test_halo_faces_are_checked():
     halo_x = ("halo", "halo") + ("periodic",) * 4
     with pytest.raises(LbmError):
