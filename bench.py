@@ -77,12 +77,15 @@ def step_kernel(storage: str, n: int) -> str:
         pair = n % 128 == 0 and env == "1"
     if not pair:
         return "aa_step_kernel"
-    return "aa_pair_kernel / aa_pair_split_kernel" if storage == "fp16dev" else "aa_pair_kernel"
+    if storage == "fp16dev":
+        quad = os.environ.get("LBM3D_QUAD") != "0"
+        return ("aa_quad_even_kernel" if quad else "aa_pair_kernel") + " / aa_pair_split_kernel"
+    return "aa_pair_kernel"
 
 
 def profiled_traffic(storage: str, n: int):
     """DRAM bytes per cell of the step kernel from the committed ncu summary."""
-    kind = "pair" if step_kernel(storage, n).startswith("aa_pair_kernel") else "step"
+    kind = "step" if step_kernel(storage, n) == "aa_step_kernel" else "pair"
     f = ROOT / "profiles" / f"aa_{kind}_{storage}_porous.txt"
     if not f.exists():
         return None

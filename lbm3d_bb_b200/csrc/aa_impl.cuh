@@ -1016,6 +1016,112 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_spl
 }
 
 
+// ---- quad kernel: even phase, FP16-deviation storage ----------------------------------
+// One thread updates four x-adjacent cells (x0 .. x0+3, x0 a multiple of 4).  In the even
+// phase every direction reads and writes the cells' own slots, for four cells one aligned
+// 8-byte word: 19 loads and 19 stores per four cells, addressing and control shared by
+// four cells.  The cells collide in pairs, from the low and the high half2 of each word,
+// and pack back to half2 at once, which bounds the live registers.
+template <bool TRT, bool FORCE>
+__global__ void __launch_bounds__(256, 2) aa_quad_even_kernel(const __grid_constant__ AAParams p,
+                                                              __half* __restrict__ A,
+                                                              const uint8_t* __restrict__ flags) {
+  using SP = StF16;
+  using C = float;
+  const Grid& g = p.g;
+  const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = x0 < g.nx && y < g.ny;
+  clear_record(p.zero_next);
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  const long long i0 = inb ? node_index(g, x0, y, z) : 0;
+  uint32_t fw = 0x01010101u * F_SOLID;
+  if (inb) fw = *reinterpret_cast<const uint32_t*>(flags + i0);
+  __half* const Ai = A + i0;
+  uint2 w[Q];
+  if (inb) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) w[d] = *reinterpret_cast<const uint2*>(Ai + p.off_rd[d]);
+  }
+  uint32_t bc[4];
+  bool fast = true, any_fluid = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t fl = (fw >> (8 * k)) & 0xFFu;
+    bc[k] = 0;
+    if (!(fl & F_SOLID)) {
+      any_fluid = true;
+      if (fl & F_NEAR) {
+        const unsigned long long lw = p.links[i0 + k];
+        bc[k] = (uint32_t)(lw & 0x3FFFFu);
+        fast = fast && bc[k] == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 &&
+               !(fl & F_SOLID_PREV);
+      }
+    }
+  }
+  if (__all_sync(0xffffffffu, !any_fluid || fast)) {
+    if (any_fluid) {
+      uint32_t out[2][Q];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int ka = 2 * h, kb = 2 * h + 1;
+        C pa[Q], pb[Q];
+        {
+          C f[Q];
+#pragma unroll
+          for (int d = 0; d < Q; d++) {
+            const uint32_t u = h ? w[d].y : w[d].x;
+            f[d] = __low2float(*reinterpret_cast<const __half2*>(&u));
+          }
+          if (!((fw >> (8 * ka)) & F_SOLID)) {
+            pair_cell<SP, false, TRT, FORCE>(p, f, pa);
+          } else {
+#pragma unroll
+            for (int d = 0; d < Q; d++) pa[d] = C(0);
+          }
+        }
+        {
+          C f[Q];
+#pragma unroll
+          for (int d = 0; d < Q; d++) {
+            const uint32_t u = h ? w[d].y : w[d].x;
+            f[d] = __high2float(*reinterpret_cast<const __half2*>(&u));
+          }
+          if (!((fw >> (8 * kb)) & F_SOLID)) {
+            pair_cell<SP, false, TRT, FORCE>(p, f, pb);
+          } else {
+#pragma unroll
+            for (int d = 0; d < Q; d++) pb[d] = C(0);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < Q; j++) {  // own slot j takes the post-collision value of opp(j)
+          const __half2 v = __floats2half2_rn(pa[opp(j)], pb[opp(j)]);
+          out[h][j] = *reinterpret_cast<const uint32_t*>(&v);
+        }
+        if (p.compute_force && (bc[ka] | bc[kb])) {
+          pair_links<SP>(p, x0 + ka, y, z, bc[ka], pa, acc);
+          pair_links<SP>(p, x0 + kb, y, z, bc[kb], pb, acc);
+          has_link = true;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < Q; j++) *reinterpret_cast<uint2*>(Ai + p.off_wr[j]) = make_uint2(out[0][j], out[1][j]);
+    }
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < 4; k++) {
+      const uint32_t fl = (fw >> (8 * k)) & 0xFFu;
+      if (inb && !(fl & F_SOLID))
+        aa_general<SP, false, TRT, FORCE>(p, A, flags, x0 + k, y, z, i0 + k, (uint8_t)fl, acc, &has_link);
+    }
+  }
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
+}
+
 // q = n / d and r = n % d for n < 2^31 through an FP64 reciprocal (exact after the
 // one-step correction; the product is off by at most one).
 __device__ __forceinline__ void divmod_rcp(const unsigned n, const int d, const double inv, unsigned& q, int& r) {
@@ -1403,10 +1509,18 @@ static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, 
   if constexpr (!FACES) {
     if (p.pair) {  // 64 x 4 threads, two cells each
       const dim3 pb(64, 4, 1), pg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 3) / 4), (unsigned)p.g.nz);
-      if constexpr (ODD && SP::DEV)
+      if constexpr (ODD && SP::DEV) {
         aa_pair_split_kernel<SP, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
-      else
+      } else if constexpr (!ODD && SP::DEV) {
+        if (p.quad) {  // 32 x 8 threads, four cells each
+          const dim3 qb(32, 8, 1), qg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 7) / 8), (unsigned)p.g.nz);
+          aa_quad_even_kernel<TRT, FORCE><<<qg, qb, 0, s>>>(p, (__half*)A, flags);
+        } else {
+          aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+        }
+      } else {
         aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+      }
       return cudaGetLastError();
     }
   }

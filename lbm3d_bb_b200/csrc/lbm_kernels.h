@@ -39,6 +39,7 @@ struct AAParams {
   // on the fast path, everything else takes the general path
   const unsigned long long* links;
   int pair;  // all axes periodic, nx % 128 == 0: two cells per thread (aa_pair_kernel)
+  int quad;  // with pair, FP16-deviation even phase: four cells per thread (aa_quad_even_kernel)
 };
 
 // Batched step over many independent config-mode domains (one launch per step).

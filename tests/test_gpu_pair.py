@@ -69,3 +69,39 @@ def test_pair_kernel_vs_oracle(gpu, oracle_lib):
     assert rel_l2(rg, ro) <= 2e-3
     assert rel_l2(ug, uo) <= 0.1
     g.check_finite()
+
+
+@pytest.mark.parametrize("steps", [6, 7])
+@pytest.mark.parametrize("collision", ["BGK", "TRT"])
+def test_quad_even_kernel_matches_pair_kernel(gpu, steps, collision):
+    """FP16-deviation even phase with four cells per thread (LBM3D_QUAD=1) against the
+    pair kernel: same populations to storage rounding, same force history."""
+    kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
+
+    def run(quad):
+        old = os.environ.get("LBM3D_QUAD")
+        os.environ["LBM3D_QUAD"] = "1" if quad else "0"
+        try:
+            rng = np.random.default_rng(11)
+            nx, ny, nz = 128, 20, 16
+            xyzr = np.concatenate([rng.uniform(0, [nx, ny, nz], (6, 3)), rng.uniform(2.0, 4.5, (6, 1))], axis=1)
+            d = Domain(nx, ny, nz, collision=collision, storage="fp16dev", faces=cases.PERIODIC, omega_p=1.0 / 0.6,
+                       accel=(1e-5, 0.0, 0.0), compute_force=True, **kw)
+            d.add_spheres(xyzr)
+            d.init_equilibrium()
+            d.step(steps)
+            return d
+        finally:
+            if old is None:
+                del os.environ["LBM3D_QUAD"]
+            else:
+                os.environ["LBM3D_QUAD"] = old
+
+    a, b = run(True), run(False)
+    try:
+        assert rel_l2(a.populations(), b.populations()) <= 1e-6
+        fa, fb = a.force_history(1, steps), b.force_history(1, steps)
+        assert np.linalg.norm(fa - fb) <= 1e-5 * np.linalg.norm(fb) + 1e-12
+    finally:
+        a.close()
+        b.close()
