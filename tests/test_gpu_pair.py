@@ -74,13 +74,14 @@ def test_pair_kernel_vs_oracle(gpu, oracle_lib):
 @pytest.mark.parametrize("steps", [6, 7])
 @pytest.mark.parametrize("collision", ["BGK", "TRT"])
 def test_quad_even_kernel_matches_pair_kernel(gpu, steps, collision):
-    """FP16-deviation even phase with four cells per thread (LBM3D_QUAD=1) against the
-    pair kernel: same populations to storage rounding, same force history."""
+    """FP16-deviation even phase with four cells per thread (LBM3D_QUAD, default on)
+    against the pair kernel: same populations to storage rounding, same force history."""
     kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
+    var = "LBM3D_QUAD"
 
     def run(quad):
-        old = os.environ.get("LBM3D_QUAD")
-        os.environ["LBM3D_QUAD"] = "1" if quad else "0"
+        old = os.environ.get(var)
+        os.environ[var] = "1" if quad else "0"
         try:
             rng = np.random.default_rng(11)
             nx, ny, nz = 128, 20, 16
@@ -93,9 +94,9 @@ def test_quad_even_kernel_matches_pair_kernel(gpu, steps, collision):
             return d
         finally:
             if old is None:
-                del os.environ["LBM3D_QUAD"]
+                del os.environ[var]
             else:
-                os.environ["LBM3D_QUAD"] = old
+                os.environ[var] = old
 
     a, b = run(True), run(False)
     try:
