@@ -37,6 +37,12 @@
 #ifndef LBM_MINB_F16
 #define LBM_MINB_F16 4
 #endif
+// blocks of BATCH_ITEM threads per SM that the batched kernel's register budget allows:
+// FP32 6 (80 registers; 2 % faster than 8 on the 512-domain sweep, 4 was slower), the
+// other storages 2 x MIN_BLOCKS
+#ifndef LBM_BATCH_MINB
+#define LBM_BATCH_MINB(SP) (sizeof(typename SP::S) == 4 ? 6 : 2 * SP::MIN_BLOCKS)
+#endif
 
 namespace lbm {
 
@@ -1149,7 +1155,7 @@ __device__ __forceinline__ void divmod_rcp(const unsigned n, const int d, const 
 // odd and skips the others (both are launched every step), so each holds one phase's
 // code.
 template <class SP, bool ODD, bool TRT, bool FORCE, bool FACES>
-__global__ void __launch_bounds__(BATCH_ITEM, 2 * SP::MIN_BLOCKS) aa_batch_kernel(const __grid_constant__ BatchParams bp) {
+__global__ void __launch_bounds__(BATCH_ITEM, LBM_BATCH_MINB(SP)) aa_batch_kernel(const __grid_constant__ BatchParams bp) {
   __shared__ AAParams sp;
   using S = typename SP::S;
   const int t = threadIdx.x;

@@ -22,6 +22,7 @@ A warm start computes the first-step residual ||u(1) - u(0)|| / ||u(0)||; above
 `fallback` the case restarts from rest (the plain method remains the fallback).
 
 Usage (one GPU):  python -m lbm3d_bb_b200.warmstart --train 256 --heldout 64 --epochs 200 --out DIR
+                  python -m lbm3d_bb_b200.warmstart --heldout 64 --eval-weights WEIGHTS.npz --out DIR
 """
 from __future__ import annotations
 
@@ -167,6 +168,7 @@ class Stepper:
                 d.init_equilibrium()
             else:
                 d.init_equilibrium(*init[k])
+        self.active = list(range(len(self.doms)))
         self.batch = Batch(self.doms)
         self.batch.capture(check)
         self.ops = Ops(stream)
@@ -193,8 +195,24 @@ class Stepper:
         return np.sqrt(nrm[:, 0] / np.maximum(nrm[:, 1], 1e-300))
 
     def advance(self):
-        self.batch.replay(1)
+        if self.batch is not None:
+            self.batch.replay(1)
         self.steps += self.check
+
+    def retire(self, done) -> None:
+        """Stops stepping the cases with done[k] true (steady or diverged): the batch and
+        its captured graph are rebuilt over the others, so the set's device time follows
+        the steps each case needs rather than the slowest case."""
+        from .batch import Batch
+
+        keep = [k for k in self.active if not done[k]]
+        if len(keep) == len(self.active):
+            return
+        self.batch.close()
+        self.active, self.batch = keep, None
+        if keep:
+            self.batch = Batch([self.doms[k] for k in keep])
+            self.batch.capture(self.check)
 
     def drags(self) -> np.ndarray:
         """Drag `check` steps ago and now, shape (cases, 2) (NaN before enough steps)."""
@@ -206,7 +224,8 @@ class Stepper:
         return out
 
     def close(self):
-        self.batch.close()
+        if self.batch is not None:
+            self.batch.close()
         for d in self.doms:
             d.close()
 
@@ -344,7 +363,7 @@ def run_to_steady_drag(params, device, stream, init=None, drag_tol=1e-5, max_ste
             st.doms[k].init_equilibrium()
     calm = np.zeros(n, int)
     steps = np.full(n, -1)
-    while (steps < 0).any() and max(d.step_count for d in st.doms) < max_steps:
+    while (steps < 0).any() and max(st.doms[k].step_count for k in st.active) < max_steps:
         st.advance()
         dr = st.drags()
         rel = np.abs(dr[:, 1] - dr[:, 0]) / np.maximum(np.abs(dr[:, 1]), 1e-12)
@@ -355,6 +374,7 @@ def run_to_steady_drag(params, device, stream, init=None, drag_tol=1e-5, max_ste
         steps[newly] = counts[newly]
         diverged = (steps < 0) & ~np.isfinite(dr[:, 1]) & (counts > st.check)
         steps[diverged] = 0
+        st.retire(steps >= 0)
     e1.record(stream)
     e1.synchronize()
     drag = np.array([float(d.force()[0]) for d in st.doms])
@@ -378,6 +398,8 @@ def main(argv=None):
     ap.add_argument("--augment", action="store_true", help="train on the three mirror images of every state too")
     ap.add_argument("--mirror-average", action="store_true", help="average the prediction over the four mirror images")
     ap.add_argument("--out", default="warmstart_out")
+    ap.add_argument("--eval-weights", default=None,
+                    help="evaluate these saved weights on the held-out seeds (no data generation or training)")
     args = ap.parse_args(argv)
     import torch
 
@@ -404,16 +426,21 @@ def _run(args, stream, out, log):
     t0 = time.perf_counter()
     train_seeds = list(range(args.train))
     held = list(range(100000, 100000 + args.heldout))
-    X, T, M, counts, rec = generate(train_seeds, 0, stream, args.max_steps, args.tol, log=log, augment=args.augment)
-    log(f"training set: {X.shape[0]} steady states of {len(train_seeds)} ({time.perf_counter() - t0:.0f} s)")
-    model = UNet3D(16, 0, stream, seed=0)
-    t1 = time.perf_counter()
-    hist = train(model, X, T, M, counts, args.epochs, args.batch, args.lr, log=log,
-                 weights=(args.rho_weight,) + CHANNEL_WEIGHTS[1:])
-    torch.cuda.synchronize()
-    train_s = time.perf_counter() - t1
-    model.save(out / "unet_c5.npz")
-    del X, T, M
+    if args.eval_weights:
+        model = UNet3D.load(args.eval_weights, 0, stream)
+        rec, hist, train_s, train_seeds = [], [float("nan")], 0.0, []
+    else:
+        X, T, M, counts, rec = generate(train_seeds, 0, stream, args.max_steps, args.tol, log=log,
+                                        augment=args.augment)
+        log(f"training set: {X.shape[0]} steady states of {len(train_seeds)} ({time.perf_counter() - t0:.0f} s)")
+        model = UNet3D(16, 0, stream, seed=0)
+        t1 = time.perf_counter()
+        hist = train(model, X, T, M, counts, args.epochs, args.batch, args.lr, log=log,
+                     weights=(args.rho_weight,) + CHANNEL_WEIGHTS[1:])
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t1
+        model.save(out / "unet_c5.npz")
+        del X, T, M
     params = [case_params(s) for s in held]
     # warm: inference (timed) + runs; rest: runs
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
