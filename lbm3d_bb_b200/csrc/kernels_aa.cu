@@ -7,7 +7,7 @@
 namespace lbm {
 
 #define LBM_AA_DECLARE_OPS(NAME)                                                                                  \
-  cudaError_t aa_step_##NAME(const AAParams& p, void* A, const uint8_t* flags, bool odd, bool trt, bool force,    \
+  cudaError_t aa_step_##NAME(const AAParams& p, void* A, const uint8_t* flags, bool odd, bool trt, int force,     \
                              bool faces, dim3 grid, dim3 block, cudaStream_t s);                                  \
   cudaError_t aa_batch_##NAME(const BatchParams& bp, bool trt, bool force, bool faces, int blocks, int* per_sm,  \
                               cudaStream_t s);                                                                    \
@@ -23,7 +23,7 @@ LBM_AA_DECLARE_OPS(fp16)
 #undef LBM_AA_DECLARE_OPS
 
 cudaError_t aa_launch_step(int storage, const AAParams& p, void* A, const uint8_t* flags, bool odd, bool trt,
-                           bool force, bool faces, dim3 grid, dim3 block, cudaStream_t s) {
+                           int force, bool faces, dim3 grid, dim3 block, cudaStream_t s) {
   switch (storage) {
     case LBM_STORE_FP32: return aa_step_fp32(p, A, flags, odd, trt, force, faces, grid, block, s);
     case LBM_STORE_FP64: return aa_step_fp64(p, A, flags, odd, trt, force, faces, grid, block, s);

@@ -205,7 +205,7 @@ __device__ __forceinline__ void block_force_reduce(double* acc, bool has, double
 // faces: some axis is not periodic (selects the kernel that keeps face nodes on the
 // fast path; the other kernel sends them to the general path).
 cudaError_t aa_launch_step(int storage, const AAParams& p, void* A, const uint8_t* flags, bool odd,
-                           bool trt, bool force, bool faces, dim3 grid, dim3 block, cudaStream_t s);
+                           bool trt, int force, bool faces, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t aa_launch_batch(int storage, const BatchParams& bp, bool trt, bool force, bool faces, int blocks,
                             cudaStream_t s);
 cudaError_t aa_batch_blocks_per_sm(int storage, bool trt, bool force, bool faces, int* per_sm);

@@ -53,12 +53,16 @@ def sphere_pose(d, n):
     return at(n - 1.0), at(n - 0.5)
 
 
-def porous_periodic(cls, n=32, count=6, rmin=2.0, rmax=4.0, tau=0.6, g=1e-5, seed=3, storage="fp64", **kw):
-    """C3 in miniature: fully periodic box, random overlapping spheres, Guo body force."""
+def porous_periodic(cls, n=32, count=6, rmin=2.0, rmax=4.0, tau=0.6, g=1e-5, seed=3, storage="fp64",
+                    accel=None, collision="BGK", **kw):
+    """C3 in miniature: fully periodic box, random overlapping spheres, Guo body force
+    (along x unless `accel` is given)."""
     rng = np.random.default_rng(seed)
     xyzr = np.concatenate([rng.uniform(0, n, (count, 3)), rng.uniform(rmin, rmax, (count, 1))], axis=1)
-    d = cls(n, n, n, collision="BGK", storage=storage, faces=PERIODIC, omega_p=1.0 / tau, accel=(g, 0.0, 0.0),
-            compute_force=False, **kw)
+    if collision == "TRT":
+        kw.setdefault("omega_m", 1.0 / (0.5 + 0.1875 / (tau - 0.5)))
+    d = cls(n, n, n, collision=collision, storage=storage, faces=PERIODIC, omega_p=1.0 / tau,
+            accel=(g, 0.0, 0.0) if accel is None else accel, compute_force=False, **kw)
     d.add_spheres(xyzr)
     d.init_equilibrium()
     return d

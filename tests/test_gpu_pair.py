@@ -106,3 +106,31 @@ def test_quad_even_kernel_matches_pair_kernel(gpu, steps, collision):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("collision", ["BGK", "TRT"])
+def test_x_only_force_matches_general_force(gpu, collision):
+    """FP16-deviation storage with an acceleration along x runs kernels that skip the
+    exact-zero y and z source terms; a 1e-30 y-acceleration selects the general kernels.
+    Same populations (to the 1e-30 terms) and force history."""
+    kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
+
+    def run(gy):
+        rng = np.random.default_rng(21)
+        nx, ny, nz = 128, 16, 16
+        xyzr = np.concatenate([rng.uniform(0, [nx, ny, nz], (5, 3)), rng.uniform(2.0, 4.0, (5, 1))], axis=1)
+        d = Domain(nx, ny, nz, collision=collision, storage="fp16dev", faces=cases.PERIODIC, omega_p=1.0 / 0.6,
+                   accel=(2e-5, gy, 0.0), compute_force=True, **kw)
+        d.add_spheres(xyzr)
+        d.init_equilibrium()
+        d.step(9)
+        return d
+
+    a, b = run(0.0), run(1e-30)
+    try:
+        assert rel_l2(a.populations(), b.populations()) <= 1e-6
+        fa, fb = a.force_history(1, 9), b.force_history(1, 9)
+        assert np.linalg.norm(fa - fb) <= 1e-6 * np.linalg.norm(fb) + 1e-12
+    finally:
+        a.close()
+        b.close()

@@ -132,9 +132,12 @@ def test_moving_sphere_trt_fp64(gpu, oracle_lib):
     _force_close(fg[:, :3], fo[:, :3], TOL_FORCE)
 
 
-def test_porous_periodic_forcing_fp64(gpu, oracle_lib):
-    g = cases.porous_periodic(Domain)
-    o = cases.porous_periodic(OracleDomain)
+@pytest.mark.parametrize("collision,accel", [("BGK", None), ("TRT", None), ("BGK", (1e-5, -4e-6, 3e-6)),
+                                             ("TRT", (0.0, 2e-6, 1e-5))])
+def test_porous_periodic_forcing_fp64(gpu, oracle_lib, collision, accel):
+    """Guo forcing along x and along a general direction, BGK and TRT, against the oracle."""
+    g = cases.porous_periodic(Domain, collision=collision, accel=accel)
+    o = cases.porous_periodic(OracleDomain, collision=collision, accel=accel)
     assert np.array_equal(g.flags()[0], o.flags()[0])
     g.step(25)
     o.step(25)
