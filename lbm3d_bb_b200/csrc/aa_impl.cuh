@@ -857,27 +857,42 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_ker
       }
       const bool plain = !solid0 && !solid1 && !(bc0 | bc1);
       const C rho0 = C(p.rho0);
+      if (ODD && plain) {
+        // both cells fluid without links: one loop without per-direction branches
+        // (FP32 odd phase 4.23 -> 3.85 ms at 512^3 on B200)
 #pragma unroll
-      for (int j = 0; j < Q; j++) {
-        if (!ODD) {  // own slots of both cells: one word
-          Pair2<S>::st(A + (long long)j * g.plane + i0, p0[opp(j)], p1[opp(j)]);
-          continue;
+        for (int j = 0; j < Q; j++) {
+          const long long o = p.off_wr[j];
+          if (cx(j) == 0) {
+            Pair2<S>::st(A + i0 + o, p0[j], p1[j]);
+          } else {
+            st_fast<SP>(A + i0 + o + (cx(j) == -1 ? fix_lo : 0), p0[j], j, rho0);
+            st_fast<SP>(A + i0 + 1 + o - (cx(j) == 1 ? fix_hi : 0), p1[j], j, rho0);
+          }
         }
-        const long long o = p.off_wr[j];
-        const int oj = opp(j);
-        if (cx(j) == 0 && plain) {
-          Pair2<S>::st(A + i0 + o, p0[j], p1[j]);
-          continue;
-        }
-        if (!solid0) {
-          long long a = i0 + o + (cx(j) == -1 ? fix_lo : 0);
-          if (j < 18 && ((bc0 >> oj) & 1u)) a = (long long)oj * g.plane + i0;
-          st_fast<SP>(A + a, p0[j], j, rho0);
-        }
-        if (!solid1) {
-          long long a = i0 + 1 + o - (cx(j) == 1 ? fix_hi : 0);
-          if (j < 18 && ((bc1 >> oj) & 1u)) a = (long long)oj * g.plane + i0 + 1;
-          st_fast<SP>(A + a, p1[j], j, rho0);
+      } else {
+#pragma unroll
+        for (int j = 0; j < Q; j++) {
+          if (!ODD) {  // own slots of both cells: one word
+            Pair2<S>::st(A + (long long)j * g.plane + i0, p0[opp(j)], p1[opp(j)]);
+            continue;
+          }
+          const long long o = p.off_wr[j];
+          const int oj = opp(j);
+          if (cx(j) == 0 && plain) {
+            Pair2<S>::st(A + i0 + o, p0[j], p1[j]);
+            continue;
+          }
+          if (!solid0) {
+            long long a = i0 + o + (cx(j) == -1 ? fix_lo : 0);
+            if (j < 18 && ((bc0 >> oj) & 1u)) a = (long long)oj * g.plane + i0;
+            st_fast<SP>(A + a, p0[j], j, rho0);
+          }
+          if (!solid1) {
+            long long a = i0 + 1 + o - (cx(j) == 1 ? fix_hi : 0);
+            if (j < 18 && ((bc1 >> oj) & 1u)) a = (long long)oj * g.plane + i0 + 1;
+            st_fast<SP>(A + a, p1[j], j, rho0);
+          }
         }
       }
       if (p.compute_force && (bc0 | bc1)) {
