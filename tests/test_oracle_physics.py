@@ -1,10 +1,12 @@
-"""Physics checks of the CPU oracle against analytic results (no reference output exists
-to pin it; these tie its config-mode physics to known solutions)."""
+"""Checks of the CPU oracle against analytic results and definitions (no reference output
+exists to pin it): config-mode physics against known solutions, and the reference-mode
+bounce-back mask and link CSR against a brute-force evaluation of their definitions."""
 import math
 
 import numpy as np
 import pytest
 
+from lbm3d_bb_b200 import abi
 from oracle.oracle import OracleDomain
 from tests import cases
 
@@ -96,3 +98,53 @@ def test_reference_mode_evolves_solid_nodes_as_virtual_fluid(oracle_lib, coll):
     solid = np.flatnonzero(ms)
     assert solid.size > 0
     assert np.max(np.abs(d.populations()[:, solid] - f0[:, solid])) > 1e-6
+
+
+def _brute_force_links(ms, shape, cxyz):
+    """mask_bb and the link CSR by their definitions (Geometry.jl:122-148, 181-262):
+    a fluid node is a bounce-back node when a neighbour inside the box (no wrap, as in
+    the reference's neighbour table, Utilities.jl:555-570) is solid; its links are those
+    directions, ascending, 1-based; bb_ptr is 1-based with bb_ptr[1] = 1."""
+    nx, ny, nz = shape
+    solid = ms.reshape(nz, ny, nx).astype(bool)
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    hit = np.zeros((19, nz, ny, nx), bool)
+    for q in range(19):
+        jx, jy, jz = x + cxyz[0][q], y + cxyz[1][q], z + cxyz[2][q]
+        inside = (jx >= 0) & (jx < nx) & (jy >= 0) & (jy < ny) & (jz >= 0) & (jz < nz)
+        s = np.zeros_like(inside)
+        s[inside] = solid[jz[inside], jy[inside], jx[inside]]
+        hit[q] = s & ~solid
+    mb = hit.any(axis=0).ravel()
+    h = hit.reshape(19, -1)
+    counts = h.sum(axis=0).astype(np.int64)
+    ptr = np.concatenate([[1], 1 + np.cumsum(counts)]).astype(np.int32)
+    node, = np.nonzero(counts)
+    lidx = np.repeat(node + 1, counts[node]).astype(np.int32)
+    dirs = np.concatenate([np.nonzero(h[:, a])[0] + 1 for a in node]).astype(np.int8) if len(node) else \
+        np.zeros(0, np.int8)
+    return mb, ptr, lidx, dirs
+
+
+@pytest.mark.parametrize("body", ["cylinder", "naca"])
+def test_link_csr_matches_its_definition(oracle_lib, body):
+    """The oracle's mask_bb and link CSR (the bit-exact contract the GPU tests hold the
+    kernels to) against a brute-force evaluation of the reference's definitions."""
+    from lbm3d_bb_b200.domain import lattice
+
+    cx, cy, cz, _, _ = lattice()
+    nx, ny, nz = 40, 24, 3
+    d = OracleDomain(nx, ny, nz, mode="reference", collision="BGK", omega_p=1.2, u_inf=(0.05, 0, 0))
+    if body == "cylinder":
+        d.add_body(abi.make_body(abi.BODY_CYLINDER_Z, (14.3, 12.1, 0.0), radius=5.2))
+    else:
+        d.add_body(abi.make_body(abi.BODY_NACA_Z, (16.0, 12.0, 0.0), chord=18.0, naca=(0.02, 0.4, 0.12)))
+    d.init_equilibrium()
+    ms, mb = d.flags()
+    ptr, lidx, dirs = d.links()
+    assert ms.sum() > 0
+    mb_ref, ptr_ref, lidx_ref, dirs_ref = _brute_force_links(ms, (nx, ny, nz), (cx, cy, cz))
+    assert np.array_equal(mb.astype(bool), mb_ref)
+    assert np.array_equal(ptr, ptr_ref)
+    assert np.array_equal(lidx, lidx_ref)
+    assert np.array_equal(dirs, dirs_ref)
