@@ -304,7 +304,7 @@ __host__ __device__ constexpr uint32_t dir_mask(int axis, int sign) {
 // incoming population d lies outside a non-periodic face.
 struct FaceLane {
   uint32_t mask;
-  bool xlo, xhi, ylo, yhi;
+  bool xlo, xhi, ylo, yhi, zlo, zhi;
 };
 
 __device__ __forceinline__ FaceLane face_lane(const Grid& g, int x, int y, int z) {
@@ -313,9 +313,10 @@ __device__ __forceinline__ FaceLane face_lane(const Grid& g, int x, int y, int z
   f.xhi = !g.per[0] && x == g.nx - 1;
   f.ylo = !g.per[1] && y == 0;
   f.yhi = !g.per[1] && y == g.ny - 1;
-  const bool zlo = !g.per[2] && z == 0, zhi = !g.per[2] && z == g.nz - 1;
+  f.zlo = !g.per[2] && z == 0;
+  f.zhi = !g.per[2] && z == g.nz - 1;
   f.mask = (f.xlo ? dir_mask(0, 1) : 0u) | (f.xhi ? dir_mask(0, -1) : 0u) | (f.ylo ? dir_mask(1, 1) : 0u) |
-           (f.yhi ? dir_mask(1, -1) : 0u) | (zlo ? dir_mask(2, 1) : 0u) | (zhi ? dir_mask(2, -1) : 0u);
+           (f.yhi ? dir_mask(1, -1) : 0u) | (f.zlo ? dir_mask(2, 1) : 0u) | (f.zhi ? dir_mask(2, -1) : 0u);
   return f;
 }
 
@@ -568,27 +569,35 @@ __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S
   // warps without a face node take the plain store loop; a warp with one runs the
   // per-direction face test on every lane (one loop, no divergence between loops)
   if (FACES && __any_sync(__activemask(), face != 0u)) {
+    // Every direction is stored without a branch; an incoming direction whose source lies
+    // outside (j in the even phase, opp(j) in the odd phase) goes to the node's own slot
+    // with a placeholder.  The face values follow, one divergent branch per face rather
+    // than one per direction, faces in ascending priority so that at edges and corners
+    // the value of face_value's rule (x face, then y, then z) is stored last.
 #pragma unroll
     for (int j = 0; j < Q; j++) {
       long long o = p.off_wr[j];
-      C v = ODD ? pst[j] : pst[opp(j)];
       if (ODD) {
         if (cx(j) == 1) o -= fix_hi;
         if (cx(j) == -1) o += fix_lo;
+        if (j < 18 && (((face | bc) >> opp(j)) & 1u)) o = (long long)opp(j) * p.g.plane;
       }
-      if (j < 18) {
-        // the incoming direction whose source lies outside: j (even), opp(j) (odd)
-        const int fd = ODD ? opp(j) : j;
-        if ((face >> fd) & 1u) {
-          v = face_value<C>(p, fd, fc.xlo, fc.xhi, fc.ylo, fc.yhi, rho, ux, uy, uz, pst,
-                            SP::DEV ? wgt<C>(fd) * rho0 : C(0));
-          if (ODD) o = (long long)fd * p.g.plane;
-        } else if (ODD && ((bc >> fd) & 1u)) {
-          o = (long long)fd * p.g.plane;
-        }
-      }
-      st_fast<SP>(base + o, v, j, rho0);
+      st_fast<SP>(base + o, ODD ? pst[j] : pst[opp(j)], j, rho0);
     }
+    const auto fix = [&](const int axis, const int sign, const bool xl, const bool xh, const bool yl, const bool yh) {
+#pragma unroll
+      for (int d = 0; d < 18; d++) {
+        if ((axis == 0 ? cx(d) : (axis == 1 ? cy(d) : cz(d))) != sign) continue;
+        const C v = face_value<C>(p, d, xl, xh, yl, yh, rho, ux, uy, uz, pst, SP::DEV ? wgt<C>(d) * rho0 : C(0));
+        st_fast<SP>(base + (long long)d * p.g.plane, v, d, rho0);
+      }
+    };
+    if (fc.zlo) fix(2, 1, false, false, false, false);
+    if (fc.zhi) fix(2, -1, false, false, false, false);
+    if (fc.ylo) fix(1, 1, false, false, true, false);
+    if (fc.yhi) fix(1, -1, false, false, false, true);
+    if (fc.xlo) fix(0, 1, true, false, false, false);
+    if (fc.xhi) fix(0, -1, false, true, false, false);
   } else {
 #pragma unroll
     for (int j = 0; j < Q; j++) {
@@ -645,7 +654,7 @@ __device__ __forceinline__ void aa_direct(const AAParams& p, typename SP::S* __r
   using C = typename SP::C;
   const Grid& g = p.g;
   const long long i = inb ? node_index(g, x, y, z) : 0;
-  FaceLane fc{0u, false, false, false, false};
+  FaceLane fc{0u, false, false, false, false, false, false};
   bool coord_fast;
   if (FACES) {
     if (inb) fc = face_lane(g, x, y, z);
