@@ -398,6 +398,8 @@ void fill_aa_params(const lbm_ctx* c, AAParams& p, bool odd) {
       p.off_rd[d] = opp(d) * pl - nb;
       p.off_wr[d] = d * pl + nb;
     }
+    p.offb_rd[d] = p.off_rd[d] * c->elem;
+    p.offb_wr[d] = p.off_wr[d] * c->elem;
   }
 }
 

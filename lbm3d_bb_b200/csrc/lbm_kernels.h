@@ -34,6 +34,8 @@ struct AAParams {
   // the 19 writes of this phase (even: own slots; odd: neighbour slots)
   long long off_rd[19];
   long long off_wr[19];
+  long long offb_rd[19];  // the same in bytes (pair kernel: one 64-bit add per access)
+  long long offb_wr[19];
   TmaCfg tma;
   // per-node link words of NEAR nodes (see near_kernel): static no-slip links stay
   // on the fast path, everything else takes the general path
