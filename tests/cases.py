@@ -61,8 +61,9 @@ def porous_periodic(cls, n=32, count=6, rmin=2.0, rmax=4.0, tau=0.6, g=1e-5, see
     xyzr = np.concatenate([rng.uniform(0, n, (count, 3)), rng.uniform(rmin, rmax, (count, 1))], axis=1)
     if collision == "TRT":
         kw.setdefault("omega_m", 1.0 / (0.5 + 0.1875 / (tau - 0.5)))
+    kw.setdefault("compute_force", False)
     d = cls(n, n, n, collision=collision, storage=storage, faces=PERIODIC, omega_p=1.0 / tau,
-            accel=(g, 0.0, 0.0) if accel is None else accel, compute_force=False, **kw)
+            accel=(g, 0.0, 0.0) if accel is None else accel, **kw)
     d.add_spheres(xyzr)
     d.init_equilibrium()
     return d
