@@ -311,15 +311,21 @@ def main():
 
     import torch
 
+    from lbm3d_bb_b200 import build
+
+    # one rank brings the in-tree libraries up to date (a no-op when they are current);
+    # the others wait for it in the process-group rendezvous
+    if rank == 0:
+        build.build()
+    torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
 
         import torch.distributed as tdist
 
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = tdist
-    torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
     dev_index = local
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
@@ -329,9 +335,6 @@ def main():
         except ValueError:
             pass
 
-    from lbm3d_bb_b200 import build
-
-    build.build()
     peak, peak_kind = load_peaks()
     n = args.size
     N = n ** 3
