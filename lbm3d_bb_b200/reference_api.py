@@ -35,7 +35,7 @@ from .domain import Domain, read_params
 F32 = np.float32
 
 COLLISIONS = ("BGK", "TRT")
-SOLID_BCS = ("SBB",)  # IBB: see DESIGN.md (the reference's IBB kernel cannot load, EPS_Q undefined)
+SOLID_BCS = ("SBB",)  # no IBB: the reference's IBB kernel cannot load (EPS_Q undefined)
 
 
 # ---- parameters ---------------------------------------------------------------------------

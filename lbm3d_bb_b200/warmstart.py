@@ -338,7 +338,7 @@ def predict(model, params: Sequence[dict], mirror_average: bool = False):
     return out
 
 
-MIN_STEPS = int(NX / U_IN)  # one flow-through time: the drag is not judged earlier
+MIN_STEPS = int(NX / U_IN)  # one flow-through time: the drag is not checked earlier
 
 
 def run_to_steady_drag(params, device, stream, init=None, drag_tol=1e-5, max_steps=40000, fallback=None):
