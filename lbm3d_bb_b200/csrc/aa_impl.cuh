@@ -1100,7 +1100,8 @@ __global__ void __launch_bounds__(256, 2) aa_quad_even_kernel(const __grid_const
   uint2 w[Q];
   if (inb) {
 #pragma unroll
-    for (int d = 0; d < Q; d++) w[d] = *reinterpret_cast<const uint2*>(Ai + p.off_rd[d]);
+    for (int d = 0; d < Q; d++)  // byte offsets: one 64-bit add per access (-2 % on B200)
+      w[d] = *reinterpret_cast<const uint2*>(reinterpret_cast<const char*>(Ai) + p.offb_rd[d]);
   }
   uint32_t bc[4];
   bool fast = true, any_fluid = false;
@@ -1165,7 +1166,8 @@ __global__ void __launch_bounds__(256, 2) aa_quad_even_kernel(const __grid_const
         }
       }
 #pragma unroll
-      for (int j = 0; j < Q; j++) *reinterpret_cast<uint2*>(Ai + p.off_wr[j]) = make_uint2(out[0][j], out[1][j]);
+      for (int j = 0; j < Q; j++)
+        *reinterpret_cast<uint2*>(reinterpret_cast<char*>(Ai) + p.offb_wr[j]) = make_uint2(out[0][j], out[1][j]);
     }
   } else {
 #pragma unroll 1
