@@ -226,49 +226,65 @@ def C_sizeof_pose() -> int:
     return ctypes.sizeof(abi.LbmPose)
 
 
-def cpu_baseline(steps_hint: int, warmup_hint: int, budget_s: float = 20.0):
-    """The CPU restatement (oracle, FP32, all host threads) on a bounded sample of the
-    same workload: a smaller periodic cube with the same sphere density."""
+CPU_N = 256        # edge of the CPU sample cube (same sphere density as the 512^3 box)
+CPU_WARMUP = 2     # untimed steps before the timed runs
+CPU_STEPS = 8      # steps per timed run
+CPU_REPEATS = 3    # timed runs; the median is reported
+
+
+def cpu_sample(n: int = CPU_N, steps: int = CPU_STEPS, repeats: int = CPU_REPEATS, warmup: int = CPU_WARMUP) -> dict:
+    """The CPU restatement (oracle, FP32, all host threads) on the fixed sample cube:
+    `warmup` untimed steps, then `repeats` timed runs of `steps` steps; median MLUPS.
+    Runs in a process without torch or CUDA (see cpu_baseline)."""
     from oracle import oracle as orc
 
     orc.build()
     cores = orc.set_threads(os.cpu_count() or 1)
-
-    def run(n, k):
-        o = orc.OracleDomain(n, n, n, precision="fp32", collision="BGK", faces=("periodic",) * 6,
-                             omega_p=1.0 / TAU, accel=(GX, 0.0, 0.0), compute_force=False)
-        o.add_spheres(sphere_table(n, max(1, round(NSPHERES * (n / 512) ** 3))))
-        o.init_equilibrium()
-        o.step(1)
+    spheres = max(1, round(NSPHERES * (n / 512) ** 3))
+    o = orc.OracleDomain(n, n, n, precision="fp32", collision="BGK", faces=("periodic",) * 6, omega_p=1.0 / TAU,
+                         accel=(GX, 0.0, 0.0), compute_force=False)
+    o.add_spheres(sphere_table(n, spheres))
+    o.init_equilibrium()
+    o.step(warmup)
+    runs = []
+    for _ in range(repeats):
         t0 = time.perf_counter()
-        o.step(k)
-        dt = time.perf_counter() - t0
-        o.close()
-        return n ** 3 * k / dt / 1e6, dt
+        o.step(steps)
+        runs.append(n ** 3 * steps / (time.perf_counter() - t0) / 1e6)
+    o.close()
+    med = statistics.median(runs)
+    return {"value": round(med, 3), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n}^3 periodic porous cube ({spheres} spheres, same density), FP32, {warmup} warm-up steps, "
+                      f"median of {repeats} runs of {steps} steps ({', '.join(f'{r:.1f}' for r in runs)} MLUPS)",
+            "n": n, "runs": [round(r, 3) for r in runs]}
 
-    probe, _ = run(96, 3)
-    cells = budget_s * probe * 1e6 / max(1, steps_hint)
-    n = int(max(64, min(512, (cells ** (1.0 / 3.0)) // 32 * 32)))
-    k = max(1, min(steps_hint, int(budget_s * probe * 1e6 / n ** 3)))
-    mlups, dt = run(n, k)
-    return {"value": round(mlups, 3), "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n}^3 periodic porous cube ({max(1, round(NSPHERES * (n / 512) ** 3))} spheres, same density), "
-                      f"{k} timed steps, FP32, {dt:.1f} s"}, n, k
+
+def cpu_baseline() -> dict:
+    """cpu_sample in a fresh interpreter that loads neither torch nor CUDA, so that both
+    arms time the same sample under the same conditions."""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--cpu-sample"], capture_output=True, text=True,
+                       env=env, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError(f"CPU sample failed ({r.returncode}): {r.stderr[-2000:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
 
 
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
-    base, n, k = cpu_baseline(args.steps, args.warmup, budget_s=min(120.0, 20.0 + 0.2 * args.steps))
+    base = cpu_baseline()
+    n = base.pop("n")
+    base.pop("runs", None)
     line = {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(n ** 3 / (base["value"] * 1e6) * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload(args.size),
+        "config": dict(workload(n), sampled_for=workload(args.size)["workload"]),
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference has no CPU path (CuArray{Float32} kernels, julia absent): the CPU restatement of "
-                "its step is timed on the host cores",
+                "its step is timed on the host cores, on a fixed sample cube of the same workload",
     }
     print(json.dumps(line), flush=True)
 
@@ -297,7 +313,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--gx", type=float, default=GX, help="body acceleration along x (workload default 1e-6)")
+    ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cpu_sample:  # child process of cpu_baseline(): no torch, no CUDA
+        print(json.dumps(cpu_sample()), flush=True)
+        return
     args.warmup = max(3, args.warmup)
     GX = args.gx
 
@@ -386,7 +406,9 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu, _, _ = cpu_baseline(args.steps, args.warmup)
+        cpu = cpu_baseline()
+        cpu.pop("n", None)
+        cpu.pop("runs", None)
 
     if rank == 0:
         line = {

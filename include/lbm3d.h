@@ -40,7 +40,9 @@ enum {
   LBM_ERR_UNSUPPORTED = 4, /* valid request this build does not implement (e.g. q=27) */
   LBM_ERR_PARSE = 5,       /* params.txt parse/validation failure */
   LBM_ERR_NUMERIC = 6,     /* non-finite populations detected by lbm_check() */
-  LBM_ERR_CAPACITY = 7     /* caller buffer too small (lbm_get_links) */
+  LBM_ERR_CAPACITY = 7,    /* caller buffer too small (lbm_get_links) */
+  LBM_ERR_TIMEOUT = 8      /* a bounded wait inside a kernel gave up; the kernel returned and the
+                              context stays usable (lbm_synchronize, lbm_wait_selftest) */
 };
 
 /* ---- enums ----------------------------------------------------------------- */
@@ -267,9 +269,20 @@ int32_t lbm_get_links(lbm_ctx* ctx, int32_t* bb_ptr, int32_t* bb_lidxs, int8_t* 
  * share the array and it keeps the last call's contents (each call overwrites every
  * entry it reads); calls that overlap on the GPU — other streams or host threads —
  * race on it.  *nnz is always written; LBM_ERR_CAPACITY when cap < nnz (link entries
- * beyond cap are not written).  Blocking: waits for nnz on the context's stream. */
+ * beyond cap are not written).  The three arrays must be device (or managed) memory of
+ * the context's device (LBM_ERR_ARG otherwise) and are written on the context's stream
+ * (lbm_set_stream): a caller that fills or reads them on another stream orders those
+ * accesses against it.  Blocking: waits for nnz on the context's stream. */
 int32_t lbm_get_links_noalloc(lbm_ctx* ctx, int32_t* d_bb_ptr, int32_t* d_bb_lidxs, int8_t* d_bb_dirs,
                               int64_t cap, int64_t* nnz);
+/* Self-test of the bounded device waits; no counterpart in the reference (its kernels
+ * never wait on the device).  Launches one block on the context's stream that waits on
+ * an mbarrier nothing arrives on, through the same bounded wait the TMA-staged step
+ * kernel uses, with a limit of `polls` polls (1 .. 2^22) instead of 2^22.  The wait
+ * gives up, the block sets the context's error word and returns with nothing in
+ * flight; the call then reports LBM_ERR_TIMEOUT, as lbm_synchronize does after a step
+ * kernel whose wait gave up, and clears the word.  Blocking. */
+int32_t lbm_wait_selftest(lbm_ctx* ctx, int32_t polls);
 /* FP64 sum of all populations over fluid nodes (reference mode: all nodes).
  * Blocking. */
 int32_t lbm_mass(lbm_ctx* ctx, double* out);

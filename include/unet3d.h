@@ -48,6 +48,12 @@ int32_t nn_conv_uses_tma(int32_t h, int32_t wd, int32_t cin, int32_t cout);
 /* Blocking: nonzero (and cleared) when a tcgen05 convolution gave up waiting for its
  * matrix multiply since the last call; its output is then not valid. */
 int32_t nn_tc_status(void* stream);
+/* Self-test of the bounded tcgen05 pipeline waits (no counterpart in the reference).
+ * One block waits on an mbarrier that no MMA commits to, through the same bounded wait
+ * the convolution kernels use, with a limit of `polls` polls (1 .. 2^22); the wait gives
+ * up, the block sets the error word and returns with nothing in flight, and the call
+ * returns the nn_tc_status of that (nonzero, word cleared).  Blocking. */
+int32_t nn_wait_selftest(int32_t polls, void* stream);
 /* Weights of the data gradient: wt[26 - tap][ci][co] = w[tap][co][ci]; then
  * din = nn_conv3d_fwd(dout, wt, NULL, din, ..., cin = cout, cout = cin, relu = 0). */
 int32_t nn_conv3d_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream);

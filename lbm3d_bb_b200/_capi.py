@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
         "lbm_halo_unpack": (i32, [vp, i32, vp]),
         "lbm_mass": (i32, [vp, P(f64)]),
         "lbm_check": (i32, [vp]),
+        "lbm_wait_selftest": (i32, [vp, i32]),
         "lbm_batch_create": (i32, [vp, i32, P(vp)]),
         "lbm_batch_destroy": (i32, [vp]),
         "lbm_batch_last_error": (C.c_char_p, [vp]),
@@ -95,7 +96,7 @@ def exported_symbols() -> list[str]:
         "lbm_device_bytes", "lbm_set_launch", "lbm_get_launch", "lbm_add_body", "lbm_add_spheres",
         "lbm_update_body", "lbm_init_equilibrium", "lbm_set_populations", "lbm_step", "lbm_step_count", "lbm_launch_count",
         "lbm_get_force", "lbm_get_force_history", "lbm_get_macros", "lbm_get_populations", "lbm_get_flags",
-        "lbm_get_links", "lbm_get_links_noalloc", "lbm_mass", "lbm_check",
+        "lbm_get_links", "lbm_get_links_noalloc", "lbm_mass", "lbm_check", "lbm_wait_selftest",
         "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_last_error", "lbm_batch_step", "lbm_batch_capture",
         "lbm_batch_replay", "lbm_batch_launch_count", "lbm_batch_synchronize",
         "lbm_halo_bytes", "lbm_halo_pack", "lbm_halo_unpack",

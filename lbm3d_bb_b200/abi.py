@@ -17,6 +17,7 @@ LBM_ERR_UNSUPPORTED = 4
 LBM_ERR_PARSE = 5
 LBM_ERR_NUMERIC = 6
 LBM_ERR_CAPACITY = 7
+LBM_ERR_TIMEOUT = 8
 
 MODE_REFERENCE = 0
 MODE_CONFIG = 1

@@ -1293,10 +1293,10 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
-// Bounded wait on an mbarrier phase: gives up after ~2^22 polls (each try_wait
-// blocks for a hardware-defined interval), returning false.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); it++) {
+// Bounded wait on an mbarrier phase: gives up after `polls` polls (default ~2^22; each
+// try_wait blocks for a hardware-defined interval), returning false.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int polls = MBAR_WAIT_POLLS) {
+  for (int it = 0; it < polls; it++) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -1306,6 +1306,21 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (ok) return true;
   }
   return false;
+}
+
+// Probe of the bounded wait above: thread 0 initialises an mbarrier that expects one
+// arrival, nothing arrives and no copy targets it, so every thread's wait gives up after
+// `polls` polls; the block then records the failure in *err as the step kernels do.
+// Nothing is in flight when the kernel returns.
+static __global__ void __launch_bounds__(32) wait_probe_kernel(const int polls, int* err) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait(smem_u32(&bar), 0u, polls);
+  if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicExch(err, 1);
 }
 
 constexpr int TMA_MAX_STAGES = 8;

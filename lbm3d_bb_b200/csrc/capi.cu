@@ -502,6 +502,7 @@ const char* lbm_status_string(int32_t s) {
     case LBM_ERR_PARSE: return "parse error";
     case LBM_ERR_NUMERIC: return "non-finite populations";
     case LBM_ERR_CAPACITY: return "capacity exceeded";
+    case LBM_ERR_TIMEOUT: return "a bounded device wait gave up";
   }
   return "unknown status";
 }
@@ -765,13 +766,26 @@ int32_t lbm_set_stream(lbm_ctx* c, void* stream) {
   return LBM_OK;
 }
 
-// Reads the device error word the step kernels set when a pipeline wait gives up.
+// Reads the device error word the step kernels set when a pipeline wait gives up; a
+// reported failure clears the word, so the context keeps working afterwards.
 static int pipeline_status(lbm_ctx* c) {
   int h = 0;
   if (c->cuda(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H err")) return LBM_ERR_CUDA;
   if (c->cuda(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize")) return LBM_ERR_CUDA;
-  if (h) return c->fail(LBM_ERR_CUDA, "a TMA pipeline wait in the step kernel gave up (error word %d)", h);
+  if (h) {
+    if (c->cuda(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream), "clear err")) return LBM_ERR_CUDA;
+    if (c->cuda(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize")) return LBM_ERR_CUDA;
+    return c->fail(LBM_ERR_TIMEOUT, "a bounded mbarrier wait in a step kernel gave up (error word %d)", h);
+  }
   return LBM_OK;
+}
+
+int32_t lbm_wait_selftest(lbm_ctx* c, int32_t polls) {
+  if (!c) return LBM_ERR_ARG;
+  if (polls < 1 || polls > MBAR_WAIT_POLLS) return c->fail(LBM_ERR_ARG, "polls %d outside [1, %d]", polls, MBAR_WAIT_POLLS);
+  if (c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  if (c->cuda(aa_launch_wait_probe(polls, c->d_err, c->stream), "wait probe")) return LBM_ERR_CUDA;
+  return pipeline_status(c);
 }
 
 int32_t lbm_synchronize(lbm_ctx* c) {
@@ -1166,6 +1180,24 @@ int32_t lbm_get_links_noalloc(lbm_ctx* c, int32_t* d_bb_ptr, int32_t* d_bb_lidxs
   if (!c || !nnz || !d_bb_ptr) return LBM_ERR_ARG;
   if (cap > 0 && (!d_bb_lidxs || !d_bb_dirs)) return c->fail(LBM_ERR_ARG, "null link arrays with cap > 0");
   if (c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) return LBM_ERR_CUDA;
+  // the kernels write the arrays directly: each must be device (or managed) memory that
+  // this context's device can address, else the call fails here instead of faulting
+  {
+    const void* arrs[3] = {d_bb_ptr, cap > 0 ? d_bb_lidxs : nullptr, cap > 0 ? d_bb_dirs : nullptr};
+    const char* names[3] = {"d_bb_ptr", "d_bb_lidxs", "d_bb_dirs"};
+    for (int k = 0; k < 3; k++) {
+      if (!arrs[k]) continue;
+      cudaPointerAttributes at{};
+      if (cudaPointerGetAttributes(&at, arrs[k]) != cudaSuccess) {
+        cudaGetLastError();  // clear the sticky-free error of an unknown pointer
+        return c->fail(LBM_ERR_ARG, "%s is not a CUDA pointer", names[k]);
+      }
+      if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+        return c->fail(LBM_ERR_ARG, "%s is not device memory (pointer type %d)", names[k], (int)at.type);
+      if (at.type == cudaMemoryTypeDevice && at.device != c->device)
+        return c->fail(LBM_ERR_ARG, "%s lives on device %d, the context on device %d", names[k], at.device, c->device);
+    }
+  }
   if (c->g.N > geo_links_noalloc_max_nodes())
     return c->fail(LBM_ERR_CAPACITY, "lbm_get_links_noalloc supports at most %lld nodes (lattice has %lld)",
                    geo_links_noalloc_max_nodes(), c->g.N);

@@ -46,6 +46,9 @@ struct AAParams {
 
 // Batched step over many independent config-mode domains (one launch per step).
 constexpr int BATCH_ITEM = 128;  // cells per work item = threads per block
+// polls after which a bounded mbarrier wait in a step kernel gives up (each try_wait
+// blocks for a hardware-defined interval: seconds in all)
+constexpr int MBAR_WAIT_POLLS = 1 << 22;
 constexpr int BATCH_LAUNCHES_PER_STEP = 3;  // even-phase and odd-phase kernels, counter advance
 
 struct BatchDom {
@@ -219,6 +222,9 @@ cudaError_t aa_launch_export(int storage, const ReadParams& p, const void* A, co
                              const ExportOut& out, dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t aa_launch_reduce(int storage, const ReadParams& p, const void* A, const uint8_t* flags,
                              double* out, dim3 grid, dim3 block, cudaStream_t s);
+// Self-test of the bounded wait: one block waits on an mbarrier that nothing arrives on,
+// gives up after `polls` polls and sets *err, exactly as a step kernel does.
+cudaError_t aa_launch_wait_probe(int polls, int* err, cudaStream_t s);
 cudaError_t aa_launch_tile_flags(const Grid& g, int tw, long long ntiles, const uint8_t* flags, uint8_t* tiles,
                                  cudaStream_t s);
 cudaError_t aa_launch_init(int storage, const InitParams& p, void* A, const uint8_t* flags, dim3 grid,

@@ -19,6 +19,7 @@
 #include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched at run time)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <mutex>
 #include <cudaTypedefs.h>
 #include <stdint.h>
 
@@ -178,9 +179,12 @@ __device__ __forceinline__ void tc_mbar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
 }
 
-__device__ __forceinline__ bool tc_mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase: false after `polls` polls (each try_wait blocks for
+// a hardware-defined interval; the default gives up after seconds).
+constexpr int TC_WAIT_POLLS = 1 << 22;
+__device__ __forceinline__ bool tc_mbar_wait(uint64_t* bar, uint32_t parity, int polls = TC_WAIT_POLLS) {
   const uint32_t a = smem_addr(bar);
-  for (int it = 0; it < (1 << 22); it++) {
+  for (int it = 0; it < polls; it++) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -190,6 +194,20 @@ __device__ __forceinline__ bool tc_mbar_wait(uint64_t* bar, uint32_t parity) {
     if (ok) return true;
   }
   return false;
+}
+
+// Probe of tc_mbar_wait: thread 0 initialises an mbarrier that expects one arrival, no
+// MMA commits to it and nothing arrives, so the wait gives up after `polls` polls and
+// the block sets the error word as a convolution CTA does.  Nothing is in flight.
+__global__ void __launch_bounds__(32) tc_wait_probe_kernel(const int polls, int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    tc_mbar_init(&bar);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = tc_mbar_wait(&bar, 0u, polls);
+  if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicExch(err, 1);
 }
 
 template <int COUT>
@@ -849,12 +867,14 @@ bool tma_tiles_fit(int h, int w) {
 }
 __device__ int g_tc_err;  // set by a tcgen05 kernel whose wait gave up
 
-// Device address of g_tc_err, looked up once per device (host code cannot use the
-// symbol itself as a device address).
+// Device address of g_tc_err, looked up once per device under a lock (host code cannot
+// use the symbol itself as a device address).
 int* tc_err_ptr() {
   static int* ptrs[64] = {nullptr};
+  static std::mutex lock;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> guard(lock);
   if (!ptrs[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_tc_err) != cudaSuccess) return nullptr;
@@ -971,6 +991,16 @@ int32_t nn_tc_status(void* stream) {
     return fail("a tcgen05 convolution gave up waiting for its MMA (error word %d)", h);
   }
   return 0;
+}
+
+int32_t nn_wait_selftest(int32_t polls, void* stream) {
+  if (polls < 1 || polls > TC_WAIT_POLLS) return fail("nn_wait_selftest: polls %d outside [1, %d]", polls, TC_WAIT_POLLS);
+  int* err = tc_err_ptr();
+  if (!err) return fail("nn_wait_selftest: no device address for the error word");
+  tc_wait_probe_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(polls, err);
+  const int rc = launched("nn_wait_selftest");
+  if (rc) return rc;
+  return nn_tc_status(stream);
 }
 
 int32_t nn_conv3d_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream) {

@@ -35,7 +35,15 @@ from .domain import Domain, read_params
 F32 = np.float32
 
 COLLISIONS = ("BGK", "TRT")
-SOLID_BCS = ("SBB",)  # no IBB: the reference's IBB kernel cannot load (EPS_Q undefined)
+# Solid boundary conditions of solid_BC!'s dispatch table (SolidBC.jl:99-123).
+# "IBB" runs the bounce-back that IBB!_gpu executes for every link of the reference's
+# bodies: it evaluates phi at x_b - c_dir (SolidBC.jl:290-292), the fluid node behind the
+# boundary node, so for a convex body (cylinder, symmetric NACA band) phi_s >= 0 holds,
+# no_brkt is true and the kernel takes its fallback (SolidBC.jl:306-319), which is the
+# SBB!_gpu formula term for term (wall point x_b - c/2, local rho, 2 w rho (c.u_w)/cs^2).
+# Its interpolating branch would need EPS_Q, defined nowhere in the reference, so it
+# cannot execute as shipped.
+SOLID_BCS = ("SBB", "IBB")
 
 
 # ---- parameters ---------------------------------------------------------------------------

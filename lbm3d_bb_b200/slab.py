@@ -217,12 +217,36 @@ class SlabExchange:
             return
         for s in self.sides:
             self.d.halo_pack(s, self.send[s])
+        # torch.distributed orders its transfers after the caller's current stream; the
+        # packs ran on the domain's stream, which may be another one: hand over with events
+        # (domain stream -> current stream before the sends, back before the unpacks)
+        dstream = self._domain_stream()
+        if dstream is not None:
+            import torch
+
+            packed = torch.cuda.Event()
+            packed.record(dstream)
+            torch.cuda.current_stream(dstream.device).wait_event(packed)
         ops = [dist.P2POp(dist.isend, self.send[s], self._peer(s), self.group) for s in sorted(self.sides, reverse=True)]
         ops += [dist.P2POp(dist.irecv, self.recv[s], self._peer(s), self.group) for s in sorted(self.sides)]
         for req in dist.batch_isend_irecv(ops):
             req.wait()
+        if dstream is not None:
+            received = torch.cuda.Event()
+            received.record(torch.cuda.current_stream(dstream.device))
+            dstream.wait_event(received)
         for s in self.sides:
             self.d.halo_unpack(s, self.recv[s])
+
+    def _domain_stream(self):
+        """The torch stream the domain enqueues on (its own, or the legacy default stream
+        when it has none); None for a CPU domain."""
+        if self.d.device == "cpu":
+            return None
+        import torch
+
+        s = getattr(self.d, "stream", None)
+        return s if s is not None else torch.cuda.default_stream(int(self.d.device))
 
 
 def run(argv=None) -> None:

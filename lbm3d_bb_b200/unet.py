@@ -60,6 +60,7 @@ def lib() -> C.CDLL:
         "nn_set_conv_engine": (i32, [i32]),
         "nn_conv_uses_tma": (i32, [i32, i32, i32, i32]),
         "nn_tc_status": (i32, [vp]),
+        "nn_wait_selftest": (i32, [i32, vp]),
         "nn_to_bf16": (i32, [vp, vp, i64, vp]),
         "nn_from_bf16": (i32, [vp, vp, i64, vp]),
     }
@@ -72,7 +73,7 @@ def lib() -> C.CDLL:
 
 
 def exported_symbols() -> list[str]:
-    return ["nn_abi_version", "nn_last_error", "nn_set_conv_engine", "nn_conv_uses_tma", "nn_tc_status", "nn_conv3d_fwd", "nn_conv3d_flip", "nn_conv3d_bwd_weight",
+    return ["nn_abi_version", "nn_last_error", "nn_set_conv_engine", "nn_conv_uses_tma", "nn_tc_status", "nn_wait_selftest", "nn_conv3d_fwd", "nn_conv3d_flip", "nn_conv3d_bwd_weight",
             "nn_bias_grad", "nn_relu_bwd", "nn_pool2", "nn_pool2_bwd", "nn_up2_concat", "nn_up2_concat_bwd",
             "nn_mse", "nn_adam", "nn_diff_norms", "nn_features_ellipsoid", "nn_unpack_fields", "nn_to_bf16",
             "nn_from_bf16"]

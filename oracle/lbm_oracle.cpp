@@ -237,11 +237,67 @@ struct Sim {
 
   void raster(const lbm_body& b, const double* c, double ct, double st, const double* rot,
               std::vector<uint8_t>& out) {
+    // 3-D shapes: only the box of radius max(radius, semi-axes) + 1 around the centre can
+    // hold inside nodes (whole axis when the box reaches around a periodic axis)
+    int lo[3] = {0, 0, 0}, hi[3] = {nx - 1, ny - 1, nz - 1};
+    const bool box = b.kind == LBM_BODY_SPHERE || b.kind == LBM_BODY_ELLIPSOID;
+    if (box) {
+      double r = b.kind == LBM_BODY_SPHERE ? b.radius : std::max(b.semi[0], std::max(b.semi[1], b.semi[2]));
+      const int n3[3] = {nx, ny, nz};
+      for (int a = 0; a < 3; a++) {
+        int l = (int)std::floor(c[a] - r - 1.0), h = (int)std::ceil(c[a] + r + 1.0);
+        if (!per[a]) {
+          l = std::max(l, 0);
+          h = std::min(h, n3[a] - 1);
+        } else if (h - l + 1 >= n3[a]) {
+          l = 0;
+          h = n3[a] - 1;
+        }
+        lo[a] = l;
+        hi[a] = h;
+      }
+    }
 #pragma omp parallel for schedule(static)
+    for (int zz = lo[2]; zz <= hi[2]; zz++)
+      for (int yy = lo[1]; yy <= hi[1]; yy++)
+        for (int xx = lo[0]; xx <= hi[0]; xx++) {
+          const int x = ((xx % nx) + nx) % nx, y = ((yy % ny) + ny) % ny, z = ((zz % nz) + nz) % nz;
+          if (inside(b, x, y, z, c, ct, st, rot)) out[idx(x, y, z)] = 1;
+        }
+  }
+
+  // Bounding box of the solid nodes, grown by one node (the links and the bounce-back
+  // flags lie inside it); a whole axis when the grown box reaches around a periodic axis.
+  // Returns false when there is no solid node.
+  bool link_box(int lo[3], int hi[3]) const {
+    int l0 = nx, l1 = ny, l2 = nz, h0 = -1, h1 = -1, h2 = -1;
+#pragma omp parallel for schedule(static) reduction(min : l0, l1, l2) reduction(max : h0, h1, h2)
     for (int z = 0; z < nz; z++)
       for (int y = 0; y < ny; y++)
         for (int x = 0; x < nx; x++)
-          if (inside(b, x, y, z, c, ct, st, rot)) out[idx(x, y, z)] = 1;
+          if (solid[idx(x, y, z)]) {
+            l0 = std::min(l0, x), h0 = std::max(h0, x);
+            l1 = std::min(l1, y), h1 = std::max(h1, y);
+            l2 = std::min(l2, z), h2 = std::max(h2, z);
+          }
+    if (h0 < 0) return false;
+    const int n3[3] = {nx, ny, nz}, L[3] = {l0, l1, l2}, H[3] = {h0, h1, h2};
+    for (int a = 0; a < 3; a++) {
+      lo[a] = L[a] - 1;
+      hi[a] = H[a] + 1;
+      if (lo[a] < 0 || hi[a] >= n3[a]) {
+        // a link may cross a periodic boundary (config mode; reference mode wraps z only
+        // in streaming, never in the link set, so clamping is exact there)
+        if (per[a] && !ref()) {
+          lo[a] = 0;
+          hi[a] = n3[a] - 1;
+        } else {
+          lo[a] = std::max(lo[a], 0);
+          hi[a] = std::min(hi[a], n3[a] - 1);
+        }
+      }
+    }
+    return true;
   }
 
   static void body_rot(const lbm_body& b, double* rot, double* ct, double* st) {
@@ -348,6 +404,7 @@ struct Sim {
     for (int i = 0; i < 9; i++) rot[i] = zero ? ((i % 4 == 0) ? 1.0 : 0.0) : pn->rot[i];
     raster(b, pn->center, pn->cos_theta, pn->sin_theta, rot, moving);
     // solid_prev keeps the flags the last completed step used (set at its end)
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < N; i++) solid[i] = static_solid[i] | moving[i];
     return LBM_OK;
   }
@@ -791,6 +848,9 @@ struct Sim {
   }
 
   int get_flags(uint8_t* ms, uint8_t* mb) const {
+    int lo[3], hi[3];
+    const bool any = link_box(lo, hi);
+#pragma omp parallel for schedule(static)
     for (int z = 0; z < nz; z++)
       for (int y = 0; y < ny; y++)
         for (int x = 0; x < nx; x++) {
@@ -798,7 +858,8 @@ struct Sim {
           if (ms) ms[i] = solid[i];
           if (mb) {
             bool hit = false;
-            if (!solid[i])
+            const bool in = any && x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2];
+            if (in && !solid[i])
               for (int d = 0; d < Q && !hit; d++) hit = is_link(x, y, z, d);
             mb[i] = hit;
           }
@@ -808,19 +869,23 @@ struct Sim {
 
   int get_links(int32_t* ptr, int32_t* lidx, int8_t* dirs, int64_t cap, int64_t* nnz) const {
     int64_t k = 0;
+    int lo[3], hi[3];
+    const bool any = link_box(lo, hi);
     if (ptr) ptr[0] = 1;
     for (int z = 0; z < nz; z++)
       for (int y = 0; y < ny; y++)
         for (int x = 0; x < nx; x++) {
           int64_t i = idx(x, y, z);
-          for (int d = 0; d < Q; d++)
-            if (is_link(x, y, z, d)) {
-              if (k < cap) {
-                if (lidx) lidx[k] = (int32_t)(i + 1);
-                if (dirs) dirs[k] = (int8_t)(d + 1);
+          const bool in = any && x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2];
+          if (in)
+            for (int d = 0; d < Q; d++)
+              if (is_link(x, y, z, d)) {
+                if (k < cap) {
+                  if (lidx) lidx[k] = (int32_t)(i + 1);
+                  if (dirs) dirs[k] = (int8_t)(d + 1);
+                }
+                k++;
               }
-              k++;
-            }
           if (ptr) ptr[i + 1] = (int32_t)(1 + k);
         }
     *nnz = k;

@@ -20,7 +20,10 @@ def test_reference_arm_line():
                 "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert key in line, key
     assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
-    assert line["config"]["workload"].startswith("porous periodic 512^3")
+    # the CPU times a fixed sample cube of the 512^3 workload, and the line names it
+    assert line["config"]["workload"].startswith(f"porous periodic {bench.CPU_N}^3")
+    assert line["config"]["sampled_for"].startswith("porous periodic 512^3")
+    assert f"median of {bench.CPU_REPEATS} runs" in line["cpu_baseline"]["sample"]
     cpu = line["cpu_baseline"]
     assert cpu["value"] == line["value"] and cpu["cores"] >= 1 and cpu["kind"] == "port" and cpu["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,

@@ -145,19 +145,30 @@ def test_porous_periodic_forcing_fp64(gpu, oracle_lib, collision, accel):
     _macros_close(g, o, TOL_FIELD)
 
 
-@pytest.mark.parametrize("storage,tol", [("fp32", 2e-5), ("fp16dev", 2e-3)])
-def test_reduced_precision_storage(gpu, oracle_lib, storage, tol):
+# Stated bounds of the reduced-precision storage forms against the FP64 oracle on the
+# miniature sphere channel (60 steps): rho and u (stacked velocity components) rel. L2,
+# and the drag averaged over steps 41-60 (contract: drag within 0.5 % of FP64).
+REDUCED = {"fp32": {"rho": 1e-6, "u": 1e-4, "drag": 1e-4},
+           "fp16dev": {"rho": 1e-4, "u": 5e-3, "drag": 5e-3}}
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16dev"])
+def test_reduced_precision_storage(gpu, oracle_lib, storage):
+    tol = REDUCED[storage]
     g = cases.sphere_channel(Domain, storage=storage)
     o = cases.sphere_channel(OracleDomain)
     g.step(60)
     o.step(60)
-    rho_g, u_g, v_g, w_g = g.macros()
-    rho_o, u_o, v_o, w_o = o.macros()
-    assert rel_l2(rho_g, rho_o) <= tol
-    assert rel_l2(u_g, u_o) <= 50 * tol
-    fd_g = g.force_history(41, 20)[:, 0]
-    fd_o = o.force_history(41, 20)[:, 0]
-    assert rel_l2(fd_g, fd_o) <= 100 * tol
+    mg, mo = g.macros(), o.macros()
+    e_rho = rel_l2(mg[0], mo[0])
+    e_u = rel_l2(np.stack(mg[1:]), np.stack(mo[1:]))
+    fd_g = g.force_history(41, 20)[:, 0].mean()
+    fd_o = o.force_history(41, 20)[:, 0].mean()
+    e_drag = abs(fd_g - fd_o) / abs(fd_o)
+    print(f"\n[{storage} vs fp64 oracle] rho {e_rho:.3e} u {e_u:.3e} drag {e_drag:.3e}")
+    assert e_rho <= tol["rho"]
+    assert e_u <= tol["u"]
+    assert e_drag <= tol["drag"]
 
 
 def _ref_case(cls, precision_kw, coll="BGK", moving=True):

@@ -13,8 +13,11 @@ pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
-def test_main_simulation_matches_oracle(gpu, oracle_lib):
-    p = ra.read_params_input(GOLDEN / "params_small_cylinder.txt")
+# params_default_reduced.txt is the reference's shipped input (input/params.txt: cylinder
+# R = 16.16, Re = 185, U_inf = 0.075, BC IBB, BGK) on a 241 x 161 x 3 box for 60 steps.
+@pytest.mark.parametrize("params_file", ["params_small_cylinder.txt", "params_default_reduced.txt"])
+def test_main_simulation_matches_oracle(gpu, oracle_lib, params_file):
+    p = ra.read_params_input(GOLDEN / params_file)
     res = ra.main_simulation(p, seed=3, macros_every_step=True)
     # the oracle, fed the same initial field and the same motion! calls
     N = p.Nx * p.Ny * p.Nz
@@ -37,7 +40,7 @@ def test_main_simulation_matches_oracle(gpu, oracle_lib):
     g = res.domain
     assert np.array_equal(g.populations(np.float32), o.populations(np.float32))
     assert np.allclose(res.CD, CD, rtol=1e-6, atol=1e-9)
-    assert len(res.snapshots) == 2 and res.snapshots[-1][0] == 40
+    assert len(res.snapshots) == 2 and res.snapshots[-1][0] == p.n_max
     rho_o, u_o, _, _ = o.macros(np.float32)
     assert np.array_equal(res.snapshots[-1][1], rho_o.ravel())
     assert np.array_equal(res.snapshots[-1][2], u_o.ravel())

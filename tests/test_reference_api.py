@@ -22,9 +22,12 @@ def test_errors_and_rank0_noops():
     with pytest.raises(ValueError, match="Unknown collision method: MRT"):
         ra.collision(None, None, *[None] * 9, 1.0, 1.0, "MRT", 10, 1)
     assert ra.collision(None, None, *[None] * 9, 1.0, 1.0, "BGK", 10, 0) is None  # master does nothing
-    with pytest.raises(ValueError, match="Unknown or unimplemented boundary condition: IBB"):
-        ra.solid_BC(None, None, None, None, None, None, None, None, None, None, "IBB", 1)
-    assert ra.solid_BC(None, None, None, None, None, None, None, None, None, None, "IBB", 0) is None
+    with pytest.raises(ValueError, match="Unknown or unimplemented boundary condition: MLS"):
+        ra.solid_BC(None, None, None, None, None, None, None, None, None, None, "MLS", 1)
+    assert ra.solid_BC(None, None, None, None, None, None, None, None, None, None, "MLS", 0) is None
+    # both entries of the reference's dispatch table are accepted (IBB runs its SBB fallback)
+    for bc in ("SBB", "IBB"):
+        assert ra.solid_BC(None, None, None, None, None, None, None, None, None, None, bc, 1) is None
     assert ra.compute_aero(1, 1, 1, None, None, None, None, None, None, None, None, None, None, 1.0, None, 0) is None
 
 

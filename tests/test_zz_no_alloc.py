@@ -74,9 +74,51 @@ def test_noalloc_reports_capacity_without_overrunning(gpu):
     assert np.array_equal(ptr, p2)
 
 
+def test_noalloc_large_lattice_matches_export_and_oracle(gpu, oracle_lib):
+    """2,097,152 nodes: more than 1024 scan blocks, so the multi-pass carry over the
+    block sums and the 64-bit block offsets run; the count is also checked against the
+    CPU oracle's CSR (a bug shared by both GPU exports would not hide there)."""
+    from oracle.oracle import OracleDomain
+
+    def make(cls):
+        d = cls(128, 128, 128, collision="BGK", faces=cases.PERIODIC, omega_p=1.0 / 0.6, compute_force=False)
+        rng = np.random.default_rng(17)
+        d.add_spheres(np.concatenate([rng.uniform(0, 128, (12, 3)), rng.uniform(4.0, 11.0, (12, 1))], axis=1))
+        d.init_equilibrium()
+        return d
+
+    d = make(Domain)
+    o = make(OracleDomain)
+    try:
+        assert d.N > 1024 * 1024
+        for _ in range(2):  # two calls in a row
+            n = _compare(d)
+        ptr, lidx, dirs = o.links()
+        st, n2, p2, l2, d2 = _noalloc(d, len(lidx))
+        assert st == abi.LBM_OK and n == n2 == len(lidx) > 0
+        assert np.array_equal(ptr, p2) and np.array_equal(lidx, l2) and np.array_equal(dirs, d2)
+    finally:
+        d.close()
+        o.close()
+
+
+def test_noalloc_rejects_host_memory(gpu):
+    d = cases.sphere_channel(Domain, storage="fp32")
+    try:
+        host = np.zeros(d.N + 1, np.int32)
+        nnz = ctypes.c_int64(-1)
+        st = lib().lbm_get_links_noalloc(d.handle, host.ctypes.data, None, None, 0, ctypes.byref(nnz))
+        assert st == abi.LBM_ERR_ARG
+        assert "not" in lib().lbm_last_error(d.handle).decode()
+    finally:
+        d.close()
+
+
 def test_noalloc_rejects_lattice_above_maximum(gpu):
     d = Domain(520, 512, 512, storage="fp16dev", compute_force=False)  # 136,314,880 > 134,217,728 nodes
-    st, n, _, _, _ = _noalloc(d, 0)
-    assert st == abi.LBM_ERR_CAPACITY
-    assert "at most 134217728 nodes" in lib().lbm_last_error(d.handle).decode()
-    d.close()
+    try:
+        st, n, _, _, _ = _noalloc(d, 0)
+        assert st == abi.LBM_ERR_CAPACITY
+        assert "at most 134217728 nodes" in lib().lbm_last_error(d.handle).decode()
+    finally:
+        d.close()
