@@ -106,8 +106,21 @@ typedef struct {
   double u_inf[3];    /* reference mode: U_inf, V_inf, W_inf (Parameters.jl:24-26) */
   double h;           /* reference mode: physical length per cell (Parameters.jl:13) */
   int32_t force_history; /* capacity of the per-step device force ring (>= 1) */
-  int32_t reserved;
+  int32_t solid_bc;   /* LBM_SOLID_* (reference mode; config mode takes LBM_SOLID_SBB) */
 } lbm_config;
+
+/* Solid boundary rule of the reference-mode step (solid_BC!, SolidBC.jl:99-153).
+ * LBM_SOLID_SBB: moving-wall simple bounce-back, SBB!_gpu (SolidBC.jl:160-210).  The
+ *   reference's "IBB" executes this same rule on its bodies: IBB!_gpu evaluates phi at
+ *   x_b - c_dir, a fluid node for a convex body, so it always takes its SBB fallback
+ *   (SolidBC.jl:290-319), and its interpolating branch needs EPS_Q, defined nowhere.
+ * LBM_SOLID_IBB: the interpolated bounce-back IBB!_gpu is written to be (SolidBC.jl:253-338):
+ *   linear interpolation (Bouzidi) with q from phi at x_b and at the solid node x_b + c_dir,
+ *   the wall point x_b + q c_dir, the fluid-side neighbour x_b - c_dir for q <= 1/2 (z wraps
+ *   as in streaming; outside the x/y range the same-node branch), and
+ *   q clamped to [1e-4, 1 - 1e-4]; links without a sign change of phi bounce back at the
+ *   half-link point x_b + c_dir/2.  Needs the moving body (cylinder or NACA band). */
+enum { LBM_SOLID_SBB = 0, LBM_SOLID_IBB = 1 };
 
 /* A rigid body. Reference shapes use centre/theta in physical units (divided by h
  * inside, as MainCore.jl:136-137 does for the node coordinates); config shapes

@@ -19,6 +19,11 @@ LBM_ERR_NUMERIC = 6
 LBM_ERR_CAPACITY = 7
 LBM_ERR_TIMEOUT = 8
 
+# solid boundary rule of the reference-mode step (lbm_config.solid_bc)
+SOLID_SBB = 0
+SOLID_IBB = 1
+SOLID_BC = {"SBB": SOLID_SBB, "IBB": SOLID_IBB}
+
 MODE_REFERENCE = 0
 MODE_CONFIG = 1
 COLL_BGK = 0
@@ -71,7 +76,7 @@ class LbmConfig(C.Structure):
         ("u_inf", C.c_double * 3),
         ("h", C.c_double),
         ("force_history", C.c_int32),
-        ("reserved", C.c_int32),
+        ("solid_bc", C.c_int32),
     ]
 
 
@@ -177,7 +182,7 @@ def make_body(kind: int, center, radius=0.0, semi=(0.0, 0.0, 0.0), rot=None, mov
 
 def make_config(nx, ny, nz, *, mode=MODE_CONFIG, collision="BGK", storage="fp32", faces=("periodic",) * 6,
                 omega_p=1.0, omega_m=None, rho0=1.0, face_u=None, accel=(0.0, 0.0, 0.0), u_inf=(0.0, 0.0, 0.0),
-                h=1.0, compute_force=True, force_history=1024) -> LbmConfig:
+                h=1.0, compute_force=True, force_history=1024, solid_bc="SBB") -> LbmConfig:
     c = LbmConfig()
     c.nx, c.ny, c.nz = int(nx), int(ny), int(nz)
     c.q = 19
@@ -200,4 +205,5 @@ def make_config(nx, ny, nz, *, mode=MODE_CONFIG, collision="BGK", storage="fp32"
         c.u_inf[a] = float(u_inf[a])
     c.h = float(h)
     c.force_history = int(force_history)
+    c.solid_bc = SOLID_BC[solid_bc] if isinstance(solid_bc, str) else int(solid_bc)
     return c

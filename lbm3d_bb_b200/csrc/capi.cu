@@ -77,6 +77,7 @@ struct lbm_ctx {
   int bx = 0, by = 0;
   bool pair = false;  // FP16 pair kernel (see aa_pair_kernel)
   bool quad = false;  // FP16-deviation even phase on aa_quad_even_kernel
+  bool packed = false;  // pair kernels collide on packed FP32 pairs (aa_pair2_kernel)
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -273,6 +274,10 @@ Kinematics kin_of(const lbm_pose& p) {
     k.vel[a] = p.vel[a];
     k.omega[a] = p.omega[a];
   }
+  // an unset angle (cos = sin = 0) is angle 0
+  const bool unset = p.cos_theta == 0.0 && p.sin_theta == 0.0;
+  k.cos_t = unset ? 1.0 : p.cos_theta;
+  k.sin_t = unset ? 0.0 : p.sin_theta;
   return k;
 }
 
@@ -313,6 +318,25 @@ RefParams ref_params(const lbm_ctx* c, const Kinematics& kin, uint8_t solid_bit)
   p.kin = kin;
   p.solid_bit = solid_bit;
   p.compute_force = 0;
+  p.solid_bc = c->cfg.solid_bc;
+  if (c->cfg.solid_bc == LBM_SOLID_IBB && c->has_moving) {
+    // the body as IBB!_gpu sees it: half-step pose, lattice units (Motion.jl:96-119)
+    const lbm_body& b = c->moving_body;
+    const float h = (float)c->cfg.h;
+    IbbGeom& q = p.ibb;
+    q.shape = b.kind;
+    q.xc = (float)kin.center[0];
+    q.yc = (float)kin.center[1];
+    q.ct = (float)kin.cos_t;
+    q.st = (float)kin.sin_t;
+    q.R = (float)b.radius / h;
+    q.chord = (float)b.chord / h;
+    q.x_le = (float)b.x_le_offset / h;
+    q.m = (float)b.naca_m;
+    q.p = (float)b.naca_p;
+    q.t = (float)b.naca_t;
+    q.x_int = (float)b.x_int;
+  }
   return p;
 }
 
@@ -619,6 +643,10 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
   if (!cfg || !out) return set_global(LBM_ERR_ARG, "null argument");
   *out = nullptr;
   if (cfg->q != 19) return set_global(LBM_ERR_UNSUPPORTED, "only q=19 (D3Q19) is implemented, got q=%d", cfg->q);
+  if (cfg->solid_bc != LBM_SOLID_SBB && cfg->solid_bc != LBM_SOLID_IBB)
+    return set_global(LBM_ERR_ARG, "solid_bc %d is not LBM_SOLID_SBB or LBM_SOLID_IBB", cfg->solid_bc);
+  if (cfg->solid_bc == LBM_SOLID_IBB && cfg->mode != LBM_MODE_REFERENCE)
+    return set_global(LBM_ERR_UNSUPPORTED, "the interpolated bounce-back is a reference-mode rule");
   if (cfg->nx < 2 || cfg->ny < 2 || cfg->nz < 1) return set_global(LBM_ERR_ARG, "bad dimensions %dx%dx%d", cfg->nx, cfg->ny, cfg->nz);
   if ((long long)cfg->nx * cfg->ny * cfg->nz >= (1LL << 31))
     return set_global(LBM_ERR_ARG, "more than 2^31-1 nodes");
@@ -727,6 +755,10 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     // kernel on B200); LBM3D_QUAD=0 keeps the pair kernel
     const char* q = std::getenv("LBM3D_QUAD");
     c->quad = c->pair && cfg->storage == LBM_STORE_FP16DEV && !(q && q[0] == '0');
+    // the collision of the two (four) cells of a thread on packed FP32 pairs, FP32 and
+    // FP16-deviation storage; LBM3D_PACKED=0 keeps the scalar pair kernels
+    const char* pk = std::getenv("LBM3D_PACKED");
+    c->packed = c->pair && cfg->storage != LBM_STORE_FP64 && !(pk && pk[0] == '0');
   }
   c->bytes += fl + ring_bytes + 64;
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);
@@ -821,6 +853,8 @@ int32_t lbm_add_body(lbm_ctx* c, const lbm_body* b) {
     for (int a = 0; a < 3; a++) c->torque_center[a] = b->center[a];
     c->any_body = true;
   }
+  if (c->cfg.solid_bc == LBM_SOLID_IBB && (!b->moving || (b->kind != LBM_BODY_CYLINDER_Z && b->kind != LBM_BODY_NACA_Z)))
+    return c->fail(LBM_ERR_UNSUPPORTED, "the interpolated bounce-back takes one moving cylinder or NACA body");
   if (b->moving) {
     if (c->has_moving) return c->fail(LBM_ERR_ARG, "at most one moving body");
     if (has_halo(c)) return c->fail(LBM_ERR_UNSUPPORTED, "slabs with halo faces take static bodies only");
@@ -993,6 +1027,7 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
       p.zero_next = next;
       p.pair = c->pair ? 1 : 0;
       p.quad = c->pair && c->quad ? 1 : 0;
+      p.packed = c->pair && c->packed ? 1 : 0;
       if (c->tma) {
         if (c->tiles_dirty) {
           c->launches++;

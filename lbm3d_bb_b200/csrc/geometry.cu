@@ -13,40 +13,11 @@
 
 #include "lbm_internal.cuh"
 #include "lbm_kernels.h"
+#include "shapes.cuh"
 
 namespace lbm {
 
 // ---- predicates -----------------------------------------------------------------------
-// NACA 4-digit band (Geometry.jl:325-356); cos(atan(s)) as 1/sqrt(1+s^2), x^4 as
-// (x*x)*(x*x) — both sides of the parity check use this form.
-__device__ void naca_upper_lower(float x, float c, float m, float p, float t, float x_int, float* yL,
-                                 float* yU) {
-  const float xbar = x / c;
-  const float xbi = fmaxf(0.0f, x_int * xbar);
-  const float rt = sqrtf(xbi);
-  const float x2 = xbi * xbi;
-  const float x3 = x2 * xbi;
-  const float x4 = x2 * x2;
-  const float yt = 5.0f * t * c * (0.2969f * rt - 0.1260f * xbi - 0.3516f * x2 + 0.2843f * x3 - 0.1015f * x4);
-  float yc, dycb;
-  if (m == 0.0f || p == 0.0f) {
-    yc = 0.0f;
-    dycb = 0.0f;
-  } else if (xbar < p) {
-    yc = m / (p * p) * (2.0f * p * xbar - xbar * xbar);
-    dycb = 2.0f * m / (p * p) * (p - xbar);
-  } else {
-    const float den = 1.0f - p;
-    const float den2 = den * den;
-    yc = m / den2 * ((1.0f - 2.0f * p) + 2.0f * p * xbar - xbar * xbar);
-    dycb = 2.0f * m / den2 * (p - xbar);
-  }
-  const float s = dycb / c;
-  const float czv = 1.0f / sqrtf(1.0f + s * s);
-  *yU = yc + yt * czv;
-  *yL = yc - yt * czv;
-}
-
 __device__ __forceinline__ double min_image(double d, int n, int periodic) {
   if (!periodic) return d;
   const double hn = 0.5 * n;

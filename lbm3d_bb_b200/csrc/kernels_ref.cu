@@ -15,6 +15,7 @@
 // plain Float32 arithmetic (no fused multiply-add) do.
 #include "lbm_internal.cuh"
 #include "lbm_kernels.h"
+#include "shapes.cuh"
 
 namespace lbm {
 
@@ -112,6 +113,60 @@ __device__ __forceinline__ double ref_sbb<double>(const RefParams& p, double fdi
   return fdir - 2.0 * wgt<double>(dir) * rho_w * cdu * 3.0;
 }
 
+// Interpolated bounce-back of link (x, dir), the solid at x + c_dir: the value of S[opp(dir)].
+// IBB!_gpu (SolidBC.jl:253-338) as it is meant to work: phi is taken at the two ends of the
+// link, the boundary node x_b and the solid node x_b + c_dir (the shipped kernel takes
+// x_b - c_dir, quirk Q3); the wall lies at x_b + q c_dir; for q <= 1/2 the second point of
+// the interpolation is the fluid-side neighbour x_b - c_dir (the shipped kernel reads
+// nbr_lli[dir, i_b], the solid node); q is clamped to [EPS_Q, 1 - EPS_Q] with EPS_Q = 1e-4
+// (a name the shipped file uses without defining it, quirk Q4).  Without a sign change of
+// phi along the link the value is the moving-wall bounce-back at the half-link point
+// x_b + c_dir/2.  Geometry in FP32 as the reference; the interpolation in T.
+constexpr float IBB_EPS_Q = 1e-4f;
+
+__device__ __forceinline__ float ibb_phi(const IbbGeom& b, float x, float y) {
+  if (b.shape == LBM_BODY_CYLINDER_Z) return phi_cylinder(x, y, b.xc, b.yc, b.R);
+  return phi_airfoil(x, y, b.xc, b.yc, b.ct, b.st, b.chord, b.m, b.p, b.t, b.x_int, b.x_le);
+}
+
+template <class T>
+__device__ __forceinline__ T ref_ibb(const RefParams& p, const T* __restrict__ Fp, T rho_w, int x, int y, int z,
+                                     long long i, int dir) {
+  const Grid& g = p.g;
+  const float h = p.h;
+  const float cxf = (float)cx(dir), cyf = (float)cy(dir);
+  const float xb = (((float)(x + 1) - 0.5f) * h) / h;  // x_lli ./ h (MainCore.jl:199-200)
+  const float yb = (((float)(y + 1) - 0.5f) * h) / h;
+  const float phib = ibb_phi(p.ibb, xb, yb);
+  const float phis = ibb_phi(p.ibb, xb + cxf, yb + cyf);
+  const float denom = phib - phis;
+  const bool no_brkt = (phib <= 0.0f) || (phis >= 0.0f) || (fabsf(denom) < 1e-8f);
+  const float q = no_brkt ? 0.5f : fminf(fmaxf(phib / denom, IBB_EPS_Q), 1.0f - IBB_EPS_Q);
+  // moving-wall term at the wall point x_w = x_b + q c_dir (uw_at_wall_lat_planar)
+  const float xw = xb + q * cxf, yw = yb + q * cyf;
+  const float rx = xw - (float)p.kin.center[0], ry = yw - (float)p.kin.center[1];
+  const float uwx = (float)p.kin.vel[0] - (float)p.kin.omega[2] * ry;
+  const float uwy = (float)p.kin.vel[1] + (float)p.kin.omega[2] * rx;
+  const float cdu = cxf * uwx + cyf * uwy;
+  const T corr = T(2) * RefT<T>::W(dir) * rho_w * T(cdu) * T(3);
+  const T fdir = Fp[(long long)dir * g.plane + i];
+  if (no_brkt) return fdir - corr;
+  const T tq = T(q);
+  if (q <= 0.5f) {
+    // fluid-side neighbour x_b - c_dir, across the periodic z axis as in streaming (the
+    // shipped nbr_lli stops at the z ends, which would send every link with c_z != 0 in the
+    // end planes of an extruded box to the same-node branch, unstable for small q);
+    // outside the x/y range the same-node branch
+    const int fx = x - cx(dir), fy = y - cy(dir), fz = (z - cz(dir) + g.nz) % g.nz;
+    if (fx >= 0 && fx < g.nx && fy >= 0 && fy < g.ny) {
+      const T ff = Fp[(long long)dir * g.plane + node_index(g, fx, fy, fz)];
+      return T(2) * tq * fdir + (T(1) - T(2) * tq) * ff - corr;
+    }
+  }
+  const T fopp = Fp[(long long)opp(dir) * g.plane + i];
+  return (T(0.5) / tq) * fdir + ((T(2) * tq - T(1)) / (T(2) * tq)) * fopp - corr;
+}
+
 // Pull S_n at node (x,y,z) from F_{n-1} and apply the solid and face conditions
 // (Streaming.jl:82-111, OtherBC.jl:65-82, SolidBC.jl:160-210, OtherBC.jl:112-169),
 // accumulating the momentum exchange (MEA.jl:93-113).
@@ -145,8 +200,12 @@ __device__ __forceinline__ void ref_pull(const RefParams& p, const T* __restrict
       if (nx_ < 0 || nx_ >= g.nx || ny_ < 0 || ny_ >= g.ny || nz_ < 0 || nz_ >= g.nz) continue;
       if (!(flags[nx_ + nxl * ny_ + nxy * nz_] & p.solid_bit)) continue;
       links |= 1u << dir;
-      const T fdir = Fp[(long long)dir * g.plane + i];
-      S[opp(dir)] = ref_sbb<T>(p, fdir, rp, x, y, dir);
+      if (p.solid_bc == LBM_SOLID_IBB) {
+        S[opp(dir)] = ref_ibb<T>(p, Fp, rp, x, y, z, i, dir);
+      } else {
+        const T fdir = Fp[(long long)dir * g.plane + i];
+        S[opp(dir)] = ref_sbb<T>(p, fdir, rp, x, y, dir);
+      }
     }
   }
   if (on_face) {

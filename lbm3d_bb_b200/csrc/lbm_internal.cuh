@@ -66,6 +66,7 @@ struct Kinematics {
   double center[3];
   double vel[3];
   double omega[3];
+  double cos_t, sin_t;  // planar angle of the pose (reference shapes: phi of the interpolated bounce-back)
 };
 
 // Domain geometry shared by the step kernels.

@@ -42,6 +42,7 @@ struct AAParams {
   const unsigned long long* links;
   int pair;  // all axes periodic, nx % 128 == 0: two cells per thread (aa_pair_kernel)
   int quad;  // with pair, FP16-deviation even phase: four cells per thread (aa_quad_even_kernel)
+  int packed;  // with pair: the collision runs on packed FP32 pairs (aa_pair2_kernel, aa_quad2_even_kernel)
 };
 
 // Batched step over many independent config-mode domains (one launch per step).
@@ -70,6 +71,15 @@ struct BatchParams {
   const long long* counter;  // batch steps completed (advanced on the device)
 };
 
+// The moving body as the interpolated bounce-back sees it (Motion.jl:104-119): planar
+// shape at the half-step pose, lattice units, FP32.
+struct IbbGeom {
+  int shape;       // LBM_BODY_CYLINDER_Z or LBM_BODY_NACA_Z
+  float xc, yc;    // half-step centre (x_c_lat, y_c_lat)
+  float ct, st;    // cos / sin of the half-step angle (c_theta_half, s_theta_half)
+  float R, chord, x_le, m, p, t, x_int;  // R_lat, chord_lat, x_le_offset_lat, NACA m p t, x_int
+};
+
 // Reference-mode step (two population buffers, virtual-fluid solids).
 struct RefParams {
   Grid g;
@@ -81,6 +91,8 @@ struct RefParams {
   int compute_force;
   double* force;
   double* zero_next;
+  int solid_bc;  // LBM_SOLID_SBB or LBM_SOLID_IBB
+  IbbGeom ibb;
 };
 
 // Read-back of the state of the last completed step.

@@ -34,13 +34,13 @@ class Domain:
     def __init__(self, nx: int, ny: int, nz: int, *, mode: str = "config", collision: str = "BGK",
                  storage: str = "fp32", faces: Sequence[str] = ("periodic",) * 6, omega_p: float = 1.0,
                  omega_m: Optional[float] = None, rho0: float = 1.0, face_u=None, accel=(0.0, 0.0, 0.0),
-                 u_inf=(0.0, 0.0, 0.0), h: float = 1.0, compute_force: bool = True, force_history: int = 1024,
+                 u_inf=(0.0, 0.0, 0.0), h: float = 1.0, compute_force: bool = True, solid_bc: str = "SBB", force_history: int = 1024,
                  device: int = 0, stream=None):
         self._L = lib()
         self.cfg = abi.make_config(nx, ny, nz, mode=abi.MODE_REFERENCE if mode == "reference" else abi.MODE_CONFIG,
                                    collision=collision, storage=storage, faces=faces, omega_p=omega_p,
                                    omega_m=omega_m, rho0=rho0, face_u=face_u, accel=accel, u_inf=u_inf, h=h,
-                                   compute_force=compute_force, force_history=force_history)
+                                   compute_force=compute_force, solid_bc=solid_bc, force_history=force_history)
         self.shape = (int(nx), int(ny), int(nz))
         self.N = int(nx) * int(ny) * int(nz)
         self.mode = mode

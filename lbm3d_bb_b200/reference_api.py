@@ -182,7 +182,10 @@ def motion(state: Domain, R, x_c, y_c, dt, h, bcstruct: SolidBCStruct, law: Moti
     bcstruct.x_c_lat = ph["x_c"] / F32(h)
     bcstruct.y_c_lat = ph["y_c"] / F32(h)
     pose_n = abi.make_pose(center=(float(pn["x_c"]), float(pn["y_c"]), 0.0), cos_theta=float(ct), sin_theta=float(st))
+    # half-time orientation for phi (the interpolated bounce-back, Motion.jl:117-119)
+    th_h = ph["theta"]
     pose_h = abi.make_pose(center=(float(bcstruct.x_c_lat), float(bcstruct.y_c_lat), 0.0),
+                           cos_theta=float(F32(np.cos(th_h))), sin_theta=float(F32(np.sin(th_h))),
                            vel=(float(bcstruct.U_c_lat), float(bcstruct.V_c_lat), 0.0),
                            omega=(0.0, 0.0, float(bcstruct.omega_lat)))
     state.update_body(pose_n, pose_h)
@@ -279,10 +282,13 @@ def _shape_body(params: LBMParams) -> abi.LbmBody:
 
 def main_simulation(params: LBMParams, *, n_max: Optional[int] = None, law: Optional[MotionLaw] = None,
                     seed: Optional[int] = 0, storage: str = "fp32", macros_every_step: bool = False,
-                    device: int = 0, rank: int = 1) -> SimulationResult:
+                    device: int = 0, rank: int = 1, interpolated_ibb: bool = False) -> SimulationResult:
     """MainCore.jl:48-395 for one partition.  The reference's unseeded 20% velocity
     noise (Initialization.jl:27-32, 70) is drawn from numpy with `seed` (None: no
-    noise).  Field snapshots are kept in memory every n_save steps instead of HDF5."""
+    noise).  Field snapshots are kept in memory every n_save steps instead of HDF5.
+    BC "IBB" runs what the reference executes (its SBB fallback, see SOLID_BCS) unless
+    `interpolated_ibb` asks for the interpolated bounce-back IBB!_gpu is written to be
+    (lbm_config.solid_bc = LBM_SOLID_IBB)."""
     n_max = params.n_max if n_max is None else n_max
     law = law or main_core_law(params)
     if params.coll not in COLLISIONS:
@@ -296,7 +302,8 @@ def main_simulation(params: LBMParams, *, n_max: Optional[int] = None, law: Opti
     fc_aero = F32(1) / (F32(0.5) * params.rho_inf * (params.U_inf * params.U_inf) * A_ref)
     dom = Domain(Nx, Ny, Nz, mode="reference", collision=params.coll, storage=storage, omega_p=float(params.omega_p),
                  omega_m=float(params.omega_m), u_inf=(float(params.U_inf), float(params.V_inf), float(params.W_inf)),
-                 h=float(params.h), force_history=max(16, min(n_max, 4096)), device=device)
+                 h=float(params.h), force_history=max(16, min(n_max, 4096)), device=device,
+                 solid_bc="IBB" if (interpolated_ibb and params.bc == "IBB") else "SBB")
     dom.add_body(_shape_body(params))
     if seed is None:
         r = np.zeros(N, np.float32)

@@ -119,6 +119,30 @@ bool inside_naca_f32(float x, float y, float xc, float yc, float ct, float st, c
   return (yL - tol <= yB) && (yB <= yU + tol);
 }
 
+// phi_cylinder_lat (Geometry.jl:365-369) and phi_airfoil_lat (Geometry.jl:372-392), FP32;
+// hypot(a, b) is evaluated as sqrt(a*a + b*b).
+float phi_cylinder_f32(float x, float y, float xc, float yc, float R) {
+  float dx = x - xc, dy = y - yc;
+  return std::sqrt(dx * dx + dy * dy) - R;
+}
+
+float phi_airfoil_f32(float xw, float yw, float xc, float yc, float ct, float st, float chord, float m,
+                      float p, float t, float x_int, float x_le_offset) {
+  float dx = xw - xc, dy = yw - yc;
+  float xB = ct * dx + st * dy;
+  float yB = -st * dx + ct * dy;
+  float xle = xB + x_le_offset;
+  if (xle < 0.0f) return std::sqrt(xle * xle + yB * yB);  // ahead of the leading edge
+  if (xle > chord) {                                      // behind the trailing edge
+    float a = xle - chord;
+    return std::sqrt(a * a + yB * yB);
+  }
+  float yL, yU;
+  naca_upper_lower_f32(xle, chord, m, p, t, x_int, &yL, &yU);
+  if ((yB >= yL) && (yB <= yU)) return -std::min(yU - yB, yB - yL);
+  return (yB > yU) ? (yB - yU) : (yL - yB);
+}
+
 double min_image(double d, int n, bool periodic) {
   if (!periodic) return d;
   double hn = 0.5 * n;
@@ -532,6 +556,57 @@ struct Sim {
     }
   }
 
+  // Interpolated bounce-back of link (x, dir), solid at x + c_dir (lbm_config.solid_bc =
+  // LBM_SOLID_IBB): IBB!_gpu (SolidBC.jl:253-338) with phi at the two ends of the link
+  // x_b and x_b + c_dir, the wall point x_b + q c_dir, the fluid-side neighbour x_b - c_dir
+  // for q <= 1/2 (across the periodic z axis as in streaming; outside the x/y range the
+  // same-node branch) and q clamped to
+  // [1e-4, 1 - 1e-4]; moving-wall bounce-back at the half-link point x_b + c_dir/2 when phi
+  // does not change sign along the link.  Body at the half-step pose (Motion.jl:96-119),
+  // lattice units, geometry in FP32; the interpolation in T.
+  T ibb_value(int x, int y, int z, int dir) const {
+    const lbm_body& b = bodies[moving_idx].b;
+    const float h = (float)cfg.h;
+    float ct = (float)pose_half.cos_theta, st = (float)pose_half.sin_theta;
+    if (pose_half.cos_theta == 0.0 && pose_half.sin_theta == 0.0) {  // unset angle: 0
+      ct = 1.0f;
+      st = 0.0f;
+    }
+    const float xc = (float)pose_half.center[0], yc = (float)pose_half.center[1];
+    auto phi = [&](float px, float py) -> float {
+      if (b.kind == LBM_BODY_CYLINDER_Z) return phi_cylinder_f32(px, py, xc, yc, (float)b.radius / h);
+      return phi_airfoil_f32(px, py, xc, yc, ct, st, (float)b.chord / h, (float)b.naca_m, (float)b.naca_p,
+                             (float)b.naca_t, (float)b.x_int, (float)b.x_le_offset / h);
+    };
+    const float cxf = (float)CX[dir], cyf = (float)CY[dir];
+    const float xb = (((float)(x + 1) - 0.5f) * h) / h;  // x_lli ./ h
+    const float yb = (((float)(y + 1) - 0.5f) * h) / h;
+    const float phib = phi(xb, yb);
+    const float phis = phi(xb + cxf, yb + cyf);
+    const float denom = phib - phis;
+    const bool no_brkt = (phib <= 0.0f) || (phis >= 0.0f) || (std::fabs(denom) < 1e-8f);
+    const float q = no_brkt ? 0.5f : std::min(std::max(phib / denom, 1e-4f), 1.0f - 1e-4f);
+    const float xw = xb + q * cxf, yw = yb + q * cyf;
+    const float rx = xw - (float)pose_half.center[0], ry = yw - (float)pose_half.center[1];
+    const float uwx = (float)pose_half.vel[0] - (float)pose_half.omega[2] * ry;
+    const float uwy = (float)pose_half.vel[1] + (float)pose_half.omega[2] * rx;
+    const float cdu = cxf * uwx + cyf * uwy;
+    const int64_t i = idx(x, y, z);
+    const T corr = T(2) * w[dir] * rho[i] * T(cdu) * T(3);
+    const T fdir = P[dir * N + i];
+    if (no_brkt) return fdir - corr;
+    const T tq = T(q);
+    if (q <= 0.5f) {
+      const int fx = x - CX[dir], fy = y - CY[dir], fz = (z - CZ[dir] + nz) % nz;  // z periodic
+      if (fx >= 0 && fx < nx && fy >= 0 && fy < ny) {
+        const T ff = P[dir * N + idx(fx, fy, fz)];
+        return T(2) * tq * fdir + (T(1) - T(2) * tq) * ff - corr;
+      }
+    }
+    const T fopp = P[OPP[dir] * N + i];
+    return (T(0.5) / tq) * fdir + ((T(2) * tq - T(1)) / (T(2) * tq)) * fopp - corr;
+  }
+
   void step_ref(double* F) {
     collide_ref();
     // streaming! (Streaming.jl:82-111) with stream_lidxs of build_stream_lists
@@ -572,7 +647,9 @@ struct Sim {
             if (!is_link(x, y, z, dir)) continue;
             int opp = OPP[dir];
             T val;
-            if (sizeof(T) == 4) {
+            if (cfg.solid_bc == LBM_SOLID_IBB && moving_idx >= 0) {
+              val = ibb_value(x, y, z, dir);
+            } else if (sizeof(T) == 4) {
               float cx = (float)CX[dir], cy = (float)CY[dir];
               float xlat = (((float)(x + 1) - 0.5f) * h) / h;  // x_lli ./ h (MainCore.jl:199)
               float ylat = (((float)(y + 1) - 0.5f) * h) / h;

@@ -148,3 +148,38 @@ def test_link_csr_matches_its_definition(oracle_lib, body):
     assert np.array_equal(ptr, ptr_ref)
     assert np.array_equal(lidx, lidx_ref)
     assert np.array_equal(dirs, dirs_ref)
+
+
+@pytest.mark.parametrize("shape", ["cyl", "naca"])
+def test_interpolated_bounce_back_keeps_the_rest_state(oracle_lib, shape):
+    """With every f* at its rest value w_d both interpolation branches of the interpolated
+    bounce-back return w_d (2q w + (1-2q) w, w/(2q) + (1 - 1/(2q)) w), so a fluid and body
+    at rest stay at rest; the same run with a uniform stream is finite and differs from SBB."""
+    F = np.float32
+
+    def make(bc, U):
+        d = OracleDomain(48, 32, 3, precision="fp64", mode="reference", collision="BGK", omega_p=1.4,
+                         u_inf=(U, 0.0, 0.0), h=1.0, solid_bc=bc)
+        if shape == "cyl":
+            d.add_body(abi.make_body(abi.BODY_CYLINDER_Z, (16.5, 16.3, 0.0), radius=5.3, moving=True))
+        else:
+            d.add_body(abi.make_body(abi.BODY_NACA_Z, (20.0, 16.2, 0.0), moving=True, chord=20.0,
+                                     naca=(float(F(0.04)), float(F(0.4)), float(F(0.12))),
+                                     x_int=float(F(1.0089304)), x_le_offset=float(F(0.25) * F(20.0))))
+        d.init_equilibrium(rho=np.ones(d.N), u=np.full(d.N, U), v=np.zeros(d.N), w=np.zeros(d.N))
+        th = -math.radians(6.0) if shape == "naca" else 0.0
+        pose = abi.make_pose(center=(16.5 if shape == "cyl" else 20.0, 16.3 if shape == "cyl" else 16.2, 0.0),
+                             theta=th)
+        d.update_body(pose, pose)
+        return d
+
+    d = make("IBB", 0.0)
+    f0 = d.populations()
+    d.step(6)
+    assert np.max(np.abs(d.populations() - f0)) < 1e-15
+    a, b = make("IBB", 0.05), make("SBB", 0.05)
+    a.step(20)
+    b.step(20)
+    fa, fb = a.populations(), b.populations()
+    assert np.all(np.isfinite(fa))
+    assert np.max(np.abs(fa - fb)) > 1e-8
