@@ -182,10 +182,10 @@ def make_body(kind: int, center, radius=0.0, semi=(0.0, 0.0, 0.0), rot=None, mov
 
 def make_config(nx, ny, nz, *, mode=MODE_CONFIG, collision="BGK", storage="fp32", faces=("periodic",) * 6,
                 omega_p=1.0, omega_m=None, rho0=1.0, face_u=None, accel=(0.0, 0.0, 0.0), u_inf=(0.0, 0.0, 0.0),
-                h=1.0, compute_force=True, force_history=1024, solid_bc="SBB") -> LbmConfig:
+                h=1.0, compute_force=True, force_history=1024, solid_bc="SBB", q=19) -> LbmConfig:
     c = LbmConfig()
     c.nx, c.ny, c.nz = int(nx), int(ny), int(nz)
-    c.q = 19
+    c.q = int(q)
     c.mode = int(mode)
     c.collision = COLLISION[collision] if isinstance(collision, str) else int(collision)
     c.storage = STORAGE[storage] if isinstance(storage, str) else int(storage)

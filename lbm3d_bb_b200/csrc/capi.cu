@@ -534,13 +534,13 @@ const char* lbm_status_string(int32_t s) {
 const char* lbm_global_error(void) { return g_error.c_str(); }
 
 int32_t lbm_lattice(int32_t q, int8_t* ocx, int8_t* ocy, int8_t* ocz, float* w, int8_t* oop) {
-  if (q != 19) return set_global(LBM_ERR_UNSUPPORTED, "only q=19 is implemented (got %d)", q);
-  for (int d = 0; d < 19; d++) {
-    if (ocx) ocx[d] = (int8_t)cx(d);
-    if (ocy) ocy[d] = (int8_t)cy(d);
-    if (ocz) ocz[d] = (int8_t)cz(d);
-    if (w) w[d] = wgt<float>(d);
-    if (oop) oop[d] = (int8_t)opp(d);
+  if (q != 19 && q != 27) return set_global(LBM_ERR_UNSUPPORTED, "q=19 or q=27 (got %d)", q);
+  for (int d = 0; d < q; d++) {
+    if (ocx) ocx[d] = (int8_t)(q == 19 ? cx(d) : cx27(d));
+    if (ocy) ocy[d] = (int8_t)(q == 19 ? cy(d) : cy27(d));
+    if (ocz) ocz[d] = (int8_t)(q == 19 ? cz(d) : cz27(d));
+    if (w) w[d] = q == 19 ? wgt<float>(d) : wgt27<float>(d);
+    if (oop) oop[d] = (int8_t)(d == q - 1 ? d : (d ^ 1));
   }
   return LBM_OK;
 }
@@ -642,7 +642,8 @@ int32_t lbm_read_params(const char* path, lbm_params* out) {
 int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
   if (!cfg || !out) return set_global(LBM_ERR_ARG, "null argument");
   *out = nullptr;
-  if (cfg->q != 19) return set_global(LBM_ERR_UNSUPPORTED, "only q=19 (D3Q19) is implemented, got q=%d", cfg->q);
+  if (cfg->q != 19 && !(cfg->q == 27 && cfg->mode == LBM_MODE_REFERENCE))
+    return set_global(LBM_ERR_UNSUPPORTED, "q=%d: D3Q19, or D3Q27 in reference mode", cfg->q);
   if (cfg->solid_bc != LBM_SOLID_SBB && cfg->solid_bc != LBM_SOLID_IBB)
     return set_global(LBM_ERR_ARG, "solid_bc %d is not LBM_SOLID_SBB or LBM_SOLID_IBB", cfg->solid_bc);
   if (cfg->solid_bc == LBM_SOLID_IBB && cfg->mode != LBM_MODE_REFERENCE)
@@ -689,6 +690,7 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
   }
   c->g.N = (long long)cfg->nx * cfg->ny * cfg->nz;
   c->g.plane = (c->g.N + 127) / 128 * 128;  // 256-byte aligned planes for every storage
+  c->g.q = cfg->q;
   c->elem = cfg->storage == LBM_STORE_FP64 ? 8 : (cfg->storage == LBM_STORE_FP16DEV ? 2 : 4);
   default_block(c);
   auto bail = [&](int rc) {
@@ -697,7 +699,7 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     return rc;
   };
   if (c->cuda(cudaSetDevice(device), "cudaSetDevice")) return bail(LBM_ERR_CUDA);
-  const size_t pop = (size_t)19 * c->g.plane * c->elem;
+  const size_t pop = (size_t)cfg->q * c->g.plane * c->elem;
   const size_t fl = (size_t)((c->g.N + 3) / 4 * 4);
   if (c->ref) {
     const size_t rb = (size_t)4 * c->g.N * c->elem;
@@ -969,7 +971,7 @@ int32_t lbm_set_populations(lbm_ctx* c, const void* f, int32_t dtype, int32_t la
   if (rc) return rc;
   DevBuf buf;
   const void* d = nullptr;
-  const size_t bytes = (size_t)19 * c->g.N * (dtype == LBM_DTYPE_F64 ? 8 : 4);
+  const size_t bytes = (size_t)c->g.q * c->g.N * (dtype == LBM_DTYPE_F64 ? 8 : 4);
   if (stage_in(c, f, bytes, where, buf, &d)) return LBM_ERR_CUDA;
   InitParams p{};
   p.g = c->g;
@@ -1137,7 +1139,7 @@ int32_t lbm_get_populations(lbm_ctx* c, void* f, int32_t dtype, int32_t layout, 
   if (dtype != LBM_DTYPE_F32 && dtype != LBM_DTYPE_F64) return c->fail(LBM_ERR_ARG, "bad dtype");
   if (layout != LBM_LAYOUT_SOA && layout != LBM_LAYOUT_REFERENCE) return c->fail(LBM_ERR_ARG, "bad layout");
   if (c->cuda(cudaSetDevice(c->device), "cudaSetDevice")) return LBM_ERR_CUDA;
-  const size_t nb = (size_t)19 * c->g.N * (dtype == LBM_DTYPE_F64 ? 8 : 4);
+  const size_t nb = (size_t)c->g.q * c->g.N * (dtype == LBM_DTYPE_F64 ? 8 : 4);
   DevBuf tmp;
   void* dst = f;
   if (where != LBM_DEVICE) {

@@ -195,6 +195,13 @@ __global__ void near_kernel(const Grid g, int mode, const Box box, uint8_t* flag
     if (fn & F_SOLID_PREV) lw |= 1ull << (18 + d);
     if (fn & F_MOVING) lw |= 1ull << (36 + d);
   }
+  if (g.q == 27) {  // D3Q27 (reference mode, no wrap): the corner neighbours count for mask_bb
+    for (int d = 18; d < 26; d++) {
+      const int nx_ = x - cx27(d), ny_ = y - cy27(d), nz_ = z - cz27(d);
+      if (nx_ < 0 || nx_ >= g.nx || ny_ < 0 || ny_ >= g.ny || nz_ < 0 || nz_ >= g.nz) continue;
+      if (flags[node_index(g, nx_, ny_, nz_)] & (F_SOLID | F_SOLID_PREV)) near = true;
+    }
+  }
   near = near && (!sc || !sp);
   flags[i] = near ? (uint8_t)(fl | F_NEAR) : (uint8_t)(fl & ~F_NEAR);
   if (links) links[i] = lw;
@@ -223,6 +230,13 @@ __device__ __forceinline__ uint32_t link_mask(const Grid& g, int mode, const uin
       nz_ = wrapc(nz_, g.nz);
     }
     if (flags[node_index(g, nx_, ny_, nz_)] & sbit) m |= 1u << d;
+  }
+  if (g.q == 27) {  // D3Q27 (reference mode, no wrap): links to the corner neighbours, bits 18..25
+    for (int d = 18; d < 26; d++) {
+      const int nx_ = x + cx27(d), ny_ = y + cy27(d), nz_ = z + cz27(d);
+      if (nx_ < 0 || nx_ >= g.nx || ny_ < 0 || ny_ >= g.ny || nz_ < 0 || nz_ >= g.nz) continue;
+      if (flags[node_index(g, nx_, ny_, nz_)] & sbit) m |= 1u << d;
+    }
   }
   return m;
 }
@@ -314,7 +328,7 @@ __global__ void fill_kernel(const Grid g, int mode, const uint8_t* __restrict__ 
   const uint32_t m = link_mask(g, mode, flags, sbit, x, y, z);
   if (!m) return;
   long long k = scan[i];
-  for (int d = 0; d < 18; d++) {
+  for (int d = 0; d < 26; d++) {  // bits 18..25: D3Q27 corners
     if ((m >> d) & 1u) {
       lidx[k] = (int32_t)(i + 1);
       dirs[k] = (int8_t)(d + 1);
@@ -443,7 +457,7 @@ __global__ void na_fill_kernel(const Grid g, int mode, const uint8_t* __restrict
   if (i < g.N) {
     ptr[i] = (int32_t)(1 + ex);
     long long k = ex;
-    for (int d = 0; d < 18; d++) {
+    for (int d = 0; d < 26; d++) {  // bits 18..25: D3Q27 corners
       if ((m >> d) & 1u) {
         if (k < cap) {  // never write past the caller's capacity
           lidx[k] = (int32_t)(i + 1);

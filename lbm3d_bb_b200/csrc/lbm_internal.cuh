@@ -34,6 +34,26 @@ __host__ __device__ __forceinline__ T wgt(int d) {
   return d < 6 ? T(1) / T(18) : (d < 18 ? T(1) / T(36) : T(1) / T(3));
 }
 
+// D3Q27 of gen_lattice_sets (Utilities.jl:962-976), 0-based: directions 0..17 are the
+// D3Q19 ones, 18..25 the corners, 26 the rest; opposite pairs (2k, 2k+1); weights 2/27,
+// 1/54, 1/216, 8/27.  The reference-mode step runs on either lattice.
+__host__ __device__ __forceinline__ constexpr int cx27(int d) {
+  constexpr int t[27] = {1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 0};
+  return t[d];
+}
+__host__ __device__ __forceinline__ constexpr int cy27(int d) {
+  constexpr int t[27] = {0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1, 0};
+  return t[d];
+}
+__host__ __device__ __forceinline__ constexpr int cz27(int d) {
+  constexpr int t[27] = {0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1, 0};
+  return t[d];
+}
+template <class T>
+__host__ __device__ __forceinline__ T wgt27(int d) {
+  return d < 6 ? T(2) / T(27) : (d < 18 ? T(1) / T(54) : (d < 26 ? T(1) / T(216) : T(8) / T(27)));
+}
+
 // ---- node flag byte ----------------------------------------------------------------
 // SOLID / MOVING describe the flags of the latest body update; SOLID_PREV /
 // MOVING_PREV those of the last completed step.  NEAR marks a node whose step
@@ -75,6 +95,7 @@ struct Grid {
   int per[3];
   long long N;      // nodes
   long long plane;  // elements between direction planes
+  int q;            // lattice: 19, or 27 (reference mode)
 };
 
 struct Box {

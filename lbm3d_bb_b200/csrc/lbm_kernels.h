@@ -135,7 +135,7 @@ __device__ __forceinline__ void put(void* base, long long k, int dtype, T v) {
 }
 
 __device__ __forceinline__ double import_value(const InitParams& p, const Grid& g, long long i, int d) {
-  const long long k = p.f_layout == LBM_LAYOUT_SOA ? (long long)d * g.N + i : (long long)d + 19LL * i;
+  const long long k = p.f_layout == LBM_LAYOUT_SOA ? (long long)d * g.N + i : (long long)d + (long long)g.q * i;
   return p.f_dtype == LBM_DTYPE_F64 ? ((const double*)p.f_in)[k] : (double)((const float*)p.f_in)[k];
 }
 

@@ -29,18 +29,18 @@ def _is_device(a) -> bool:
 
 
 class Domain:
-    """One D3Q19 lattice of nx*ny*nz nodes (x fastest) on one GPU."""
+    """One lattice (D3Q19; D3Q27 in reference mode) of nx*ny*nz nodes (x fastest) on one GPU."""
 
     def __init__(self, nx: int, ny: int, nz: int, *, mode: str = "config", collision: str = "BGK",
                  storage: str = "fp32", faces: Sequence[str] = ("periodic",) * 6, omega_p: float = 1.0,
                  omega_m: Optional[float] = None, rho0: float = 1.0, face_u=None, accel=(0.0, 0.0, 0.0),
-                 u_inf=(0.0, 0.0, 0.0), h: float = 1.0, compute_force: bool = True, solid_bc: str = "SBB", force_history: int = 1024,
+                 u_inf=(0.0, 0.0, 0.0), h: float = 1.0, compute_force: bool = True, solid_bc: str = "SBB", force_history: int = 1024, q: int = 19,
                  device: int = 0, stream=None):
         self._L = lib()
         self.cfg = abi.make_config(nx, ny, nz, mode=abi.MODE_REFERENCE if mode == "reference" else abi.MODE_CONFIG,
                                    collision=collision, storage=storage, faces=faces, omega_p=omega_p,
                                    omega_m=omega_m, rho0=rho0, face_u=face_u, accel=accel, u_inf=u_inf, h=h,
-                                   compute_force=compute_force, solid_bc=solid_bc, force_history=force_history)
+                                   compute_force=compute_force, solid_bc=solid_bc, force_history=force_history, q=q)
         self.shape = (int(nx), int(ny), int(nz))
         self.N = int(nx) * int(ny) * int(nz)
         self.mode = mode
@@ -180,12 +180,13 @@ class Domain:
         self._check(self._L.lbm_get_macros(self._h, _ptr(rho), _ptr(u), _ptr(v), _ptr(w), dt, abi.DEVICE))
 
     def populations(self, dtype=np.float64, layout: str = "soa") -> np.ndarray:
-        """S_n as (19, N) for layout 'soa' or (N, 19) for 'reference' (f[d + 19*node])."""
+        """S_n as (q, N) for layout 'soa' or (N, q) for 'reference' (f[d + q*node])."""
         lay = abi.LAYOUT_SOA if layout == "soa" else abi.LAYOUT_REFERENCE
-        out = np.empty(19 * self.N, dtype=dtype)
+        q = self.cfg.q
+        out = np.empty(q * self.N, dtype=dtype)
         dt = abi.DTYPE_F64 if dtype == np.float64 else abi.DTYPE_F32
         self._check(self._L.lbm_get_populations(self._h, out.ctypes.data, dt, lay, abi.HOST))
-        return out.reshape(19, self.N) if lay == abi.LAYOUT_SOA else out.reshape(self.N, 19)
+        return out.reshape(q, self.N) if lay == abi.LAYOUT_SOA else out.reshape(self.N, q)
 
     def populations_into(self, f, layout: str = "soa") -> None:
         lay = abi.LAYOUT_SOA if layout == "soa" else abi.LAYOUT_REFERENCE
@@ -227,14 +228,14 @@ def read_params(path: str) -> abi.LbmParams:
     return p
 
 
-def lattice():
-    """(cx, cy, cz, w, opp) of D3Q19 from the library."""
-    cx = np.empty(19, np.int8)
-    cy = np.empty(19, np.int8)
-    cz = np.empty(19, np.int8)
-    w = np.empty(19, np.float32)
-    op = np.empty(19, np.int8)
-    check(lib().lbm_lattice(19, cx.ctypes.data, cy.ctypes.data, cz.ctypes.data, w.ctypes.data, op.ctypes.data))
+def lattice(q: int = 19):
+    """(cx, cy, cz, w, opp) of D3Q19 (q=19) or D3Q27 (q=27) from the library."""
+    cx = np.empty(q, np.int8)
+    cy = np.empty(q, np.int8)
+    cz = np.empty(q, np.int8)
+    w = np.empty(q, np.float32)
+    op = np.empty(q, np.int8)
+    check(lib().lbm_lattice(q, cx.ctypes.data, cy.ctypes.data, cz.ctypes.data, w.ctypes.data, op.ctypes.data))
     return cx, cy, cz, w, op
 
 

@@ -91,12 +91,11 @@ def read_params_input(path: str) -> LBMParams:
 
 def gen_lattice_sets(params: LBMParams):
     """(c_x, c_y, c_z, W, bbOpp) with the reference's 1-based bbOpp (Utilities.jl:949-960)."""
-    if params.q != 19:
-        raise ValueError("Invalid q value!" if params.q not in (3, 27) else
-                         f"q={params.q}: only D3Q19 is implemented by liblbm3d")
+    if params.q not in (19, 27):
+        raise ValueError("Invalid q value!" if params.q != 3 else "q=3: D1Q3 is not implemented by liblbm3d")
     from .domain import lattice
 
-    cx, cy, cz, w, op = lattice()
+    cx, cy, cz, w, op = lattice(params.q)
     return cx, cy, cz, w, (op + 1).astype(np.int8)
 
 
@@ -303,7 +302,7 @@ def main_simulation(params: LBMParams, *, n_max: Optional[int] = None, law: Opti
     dom = Domain(Nx, Ny, Nz, mode="reference", collision=params.coll, storage=storage, omega_p=float(params.omega_p),
                  omega_m=float(params.omega_m), u_inf=(float(params.U_inf), float(params.V_inf), float(params.W_inf)),
                  h=float(params.h), force_history=max(16, min(n_max, 4096)), device=device,
-                 solid_bc="IBB" if (interpolated_ibb and params.bc == "IBB") else "SBB")
+                 solid_bc="IBB" if (interpolated_ibb and params.bc == "IBB") else "SBB", q=params.q)
     dom.add_body(_shape_body(params))
     if seed is None:
         r = np.zeros(N, np.float32)
@@ -329,7 +328,7 @@ def main_simulation(params: LBMParams, *, n_max: Optional[int] = None, law: Opti
         motion(dom, params.R, params.x_c, params.y_c, params.dt, params.h, bcs, law, n, rank)
         collision(f_old, f_new, rho, u, v, w, c_x, c_y, c_z, wvec, bbOpp, params.omega_p, params.omega_m,
                   params.coll, N, rank)
-        streaming(f_new, f_old, None, None, 19, N, rank)
+        streaming(f_new, f_old, None, None, params.q, N, rank)
         periodic_BC(f_old, f_new, None, None, None, rank)
         solid_BC(f_old, f_new, rho, wvec, c_x, c_y, None, None, bcs, params, params.bc, rank)
         velocity_BC(f_old, f_new, None, None, None, None, bbOpp, c_x, c_y, c_z, wvec, rho, u, v, w,

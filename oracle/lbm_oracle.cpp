@@ -59,6 +59,17 @@ T weight(int d) {  // Float32.(W) of the rationals 1//18, 1//36, 1//3
   return d < 6 ? T(1) / T(18) : (d < 18 ? T(1) / T(36) : T(1) / T(3));
 }
 
+// D3Q27 of gen_lattice_sets, Utilities.jl:962-976, 0-based: the D3Q19 directions first,
+// then the eight corners, rest last; opposite pairs (2k, 2k+1).
+const int CX27[27] = {1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 0};
+const int CY27[27] = {0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1, 0};
+const int CZ27[27] = {0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1, 0};
+
+template <class T>
+T weight27(int d) {  // Float32.(W) of 2//27, 1//54, 1//216, 8//27
+  return d < 6 ? T(2) / T(27) : (d < 18 ? T(1) / T(54) : (d < 26 ? T(1) / T(216) : T(8) / T(27)));
+}
+
 struct Body {
   lbm_body b;
 };
@@ -182,7 +193,10 @@ struct Sim {
   bool have_pose = false;
   int64_t nstep = 0;
   std::vector<double> force_hist;  // 6 per step
-  T w[19];
+  // the lattice of this run (these members shadow the D3Q19 tables at namespace scope)
+  int Q = 19;
+  int CX[27], CY[27], CZ[27], OPP[27];
+  T w[27];
 
   bool ref() const { return cfg.mode == LBM_MODE_REFERENCE; }
 
@@ -191,9 +205,16 @@ struct Sim {
     nx = c->nx;
     ny = c->ny;
     nz = c->nz;
-    if (c->q != 19) {
-      err = "only q=19 is implemented";
+    if (c->q != 19 && !(c->q == 27 && c->mode == LBM_MODE_REFERENCE)) {
+      err = "q=19, or q=27 in reference mode";
       return LBM_ERR_UNSUPPORTED;
+    }
+    Q = c->q;
+    for (int d = 0; d < Q; d++) {
+      CX[d] = Q == 19 ? ::CX[d] : CX27[d];
+      CY[d] = Q == 19 ? ::CY[d] : CY27[d];
+      CZ[d] = Q == 19 ? ::CZ[d] : CZ27[d];
+      OPP[d] = d == Q - 1 ? d : (d ^ 1);
     }
     if (nx < 2 || ny < 2 || nz < 1) {
       err = "bad dimensions";
@@ -208,7 +229,7 @@ struct Sim {
       for (int a = 0; a < 3; a++) per[a] = (c->face[2 * a] == LBM_FACE_PERIODIC);
       if (cfg.h == 0.0) cfg.h = 1.0;
     }
-    for (int d = 0; d < Q; d++) w[d] = weight<T>(d);
+    for (int d = 0; d < Q; d++) w[d] = Q == 19 ? weight<T>(d) : weight27<T>(d);
     S.assign((size_t)Q * N, T(0));
     P.assign((size_t)Q * N, T(0));
     if (ref()) {

@@ -69,12 +69,12 @@ class OracleDomain:
     def __init__(self, nx: int, ny: int, nz: int, *, precision: str = "fp64", mode: str = "config",
                  collision: str = "BGK", faces: Sequence[str] = ("periodic",) * 6, omega_p: float = 1.0,
                  omega_m: Optional[float] = None, rho0: float = 1.0, face_u=None, accel=(0.0, 0.0, 0.0),
-                 u_inf=(0.0, 0.0, 0.0), h: float = 1.0, compute_force: bool = True, solid_bc: str = "SBB", **_ignored):
+                 u_inf=(0.0, 0.0, 0.0), h: float = 1.0, compute_force: bool = True, solid_bc: str = "SBB", q: int = 19, **_ignored):
         self._L = lib()
         self.cfg = abi.make_config(nx, ny, nz, mode=abi.MODE_REFERENCE if mode == "reference" else abi.MODE_CONFIG,
                                    collision=collision, storage="fp64", faces=faces, omega_p=omega_p,
                                    omega_m=omega_m, rho0=rho0, face_u=face_u, accel=accel, u_inf=u_inf, h=h,
-                                   compute_force=compute_force, solid_bc=solid_bc)
+                                   compute_force=compute_force, solid_bc=solid_bc, q=q)
         self.shape = (int(nx), int(ny), int(nz))
         self.N = int(nx) * int(ny) * int(nz)
         self._h = self._L.orc_create(C.byref(self.cfg), 1 if precision == "fp64" else 0)
@@ -118,7 +118,7 @@ class OracleDomain:
     def set_populations(self, f, layout="soa"):
         a = np.asarray(f, dtype=np.float64)
         if layout != "soa":
-            a = a.reshape(self.N, 19).T
+            a = a.reshape(self.N, self.cfg.q).T
         a = np.ascontiguousarray(a)
         self._check(self._L.orc_set_populations(self._h, a.ctypes.data))
 
@@ -145,9 +145,9 @@ class OracleDomain:
         return tuple(o.astype(dtype).reshape(nz, ny, nx) for o in outs)
 
     def populations(self, dtype=np.float64, layout="soa"):
-        out = np.empty(19 * self.N)
+        out = np.empty(self.cfg.q * self.N)
         self._check(self._L.orc_get_populations(self._h, out.ctypes.data))
-        out = out.reshape(19, self.N).astype(dtype)
+        out = out.reshape(self.cfg.q, self.N).astype(dtype)
         return out if layout == "soa" else np.ascontiguousarray(out.T)
 
     def flags(self):

@@ -72,6 +72,36 @@ def test_lattice_constants():
         assert (cx[o], cy[o], cz[o]) == (-cx[d], -cy[d], -cz[d])
 
 
+def test_lattice_d3q27_constants_and_isotropy():
+    from lbm3d_bb_b200 import lattice
+
+    cx, cy, cz, w, op = lattice(27)
+    # gen_lattice_sets D3Q27 (Utilities.jl:962-976), 0-based opposites
+    assert list(cx) == [1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 0]
+    assert list(cy) == [0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1, 0]
+    assert list(cz) == [0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1, 0]
+    assert list(op) == [d ^ 1 for d in range(26)] + [26]
+    F = np.float32
+    assert w[0] == F(2) / F(27) and w[6] == F(1) / F(54) and w[18] == F(1) / F(216) and w[26] == F(8) / F(27)
+    c = np.stack([cx, cy, cz]).astype(np.float64)
+    wd = w.astype(np.float64)
+    # all 27 velocities distinct; the moments of a lattice with c_s^2 = 1/3
+    assert len({(a, b, e) for a, b, e in zip(cx, cy, cz)}) == 27
+    assert abs(wd.sum() - 1) < 1e-6
+    assert np.allclose(c @ wd, 0, atol=1e-7)
+    assert np.allclose((c * wd) @ c.T, np.eye(3) / 3, atol=1e-7)
+    for d in range(27):
+        o = op[d]
+        assert (cx[o], cy[o], cz[o]) == (-cx[d], -cy[d], -cz[d])
+    from lbm3d_bb_b200 import reference_api as ra
+
+    p = ra.read_params_input(Path(__file__).resolve().parent / "golden" / "params_d3q27.txt")
+    assert p.q == 27
+    _, _, _, _, bbopp = ra.gen_lattice_sets(p)
+    assert list(bbopp) == [2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17, 20, 19, 22, 21, 24, 23, 26,
+                           25, 27]
+
+
 def _julia_read_params(path):
     """Restatement of read_params_input + LBMParams in Python/float32 (test oracle)."""
     F = np.float32

@@ -79,6 +79,34 @@ def test_slabs_reproduce_the_undivided_box(parts, steps, storage, collision, fac
             s.close()
 
 
+@pytest.mark.parametrize("parts,steps,collision,faces", [
+    (2, 9, "BGK", cases.PERIODIC),
+    (3, 10, "TRT", CHANNEL),
+])
+def test_slabs_match_the_oracle(gpu, oracle_lib, parts, steps, collision, faces):
+    """The decomposed run against the CPU oracle of the whole box (FP64): owned-node
+    populations, the summed force history and the density."""
+    from oracle.oracle import OracleDomain
+
+    o = OracleDomain(NX, NY, NZ, precision="fp64", **_kw("fp64", collision, faces))
+    o.add_spheres(SPHERES)
+    o.init_equilibrium()
+    o.step(steps)
+    g = _slabs(parts, steps, "fp64", collision, faces)
+    try:
+        f_slab = np.concatenate([s.populations() for s in g.slabs], axis=1)
+        assert rel_l2(f_slab, o.populations().reshape(19, NZ, NY, NX)) <= 1e-12
+        fs = np.stack([g.force(k) for k in range(1, steps + 1)])[:, :3]
+        fo = o.force_history(1, steps)[:, :3]
+        assert np.linalg.norm(fs - fo) <= 1e-9 * np.linalg.norm(fo) + 1e-11
+        rho = np.concatenate([s.macros()[0] for s in g.slabs], axis=0)
+        assert rel_l2(rho, o.macros()[0]) <= 1e-12
+    finally:
+        o.close()
+        for s in g.slabs:
+            s.close()
+
+
 @pytest.mark.parametrize("storage,parts,steps", [("fp32", 2, 7), ("fp16dev", 3, 8), ("fp64", 2, 6)])
 def test_slabs_on_the_pair_kernel(storage, parts, steps):
     """Periodic x and y with nx a multiple of 128: slabs run the pair kernel (FP32 and
