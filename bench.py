@@ -218,6 +218,57 @@ def time_e2e(n: int, storage: str, steps: int, warmup: int, device: int, stream,
     return ms, h2d, d2h, last
 
 
+def time_moving_body(steps: int, warmup: int, device: int, stream, dist, storage: str = "fp32"):
+    """The oscillating-sphere channel (192x96x96, TRT tau+ 0.56, Lambda 3/16, inlet u_x 0.03,
+    sphere r 10 at x 64, z 48, y_c(t) = 48 + 8 sin(2 pi t / 2000)) through the public API: every
+    step the host evaluates the motion law and passes the two poses (lbm_update_body), and the
+    step rebuilds the moving body's flags and links in its box, refills the uncovered nodes
+    and runs the face-aware step kernel (the reference's per-step motion!, Motion.jl:41-122,
+    plus collision through the momentum exchange)."""
+    import torch
+
+    from lbm3d_bb_b200 import Domain, abi
+
+    tau_p, lam = 0.56, 3.0 / 16.0
+    d = Domain(192, 96, 96, collision="TRT", storage=storage, faces=("inlet", "outflow", "wall", "wall", "wall", "wall"),
+               omega_p=1.0 / tau_p, omega_m=1.0 / (0.5 + lam / (tau_p - 0.5)),
+               face_u=[(0.03, 0.0, 0.0)] + [(0.0, 0.0, 0.0)] * 5, force_history=4096, device=device, stream=stream)
+    d.add_body(abi.make_body(abi.BODY_SPHERE, (64.0, 48.0, 48.0), radius=10.0, moving=True))
+    d.init_equilibrium()
+    w = 2.0 * math.pi / 2000.0
+
+    def poses(n):
+        def at(t):
+            return abi.make_pose(center=(64.0, 48.0 + 8.0 * math.sin(w * t), 48.0),
+                                 vel=(0.0, 8.0 * w * math.cos(w * t), 0.0))
+        return at(n - 1.0), at(n - 0.5)
+
+    n = 0
+    for _ in range(warmup):
+        n += 1
+        d.update_body(*poses(n))
+        d.step(1)
+    d.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = d.launch_count
+    ev0.record(stream)
+    for _ in range(steps):
+        n += 1
+        d.update_body(*poses(n))
+        d.step(1)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = d.launch_count - l0
+    d.check_finite()
+    d.close()
+    return ms, launches, 192 * 96 * 96
+
+
 def C_sizeof_pose() -> int:
     import ctypes
 
@@ -312,6 +363,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--no-moving", action="store_true", help="skip the moving-body channel line")
     ap.add_argument("--gx", type=float, default=GX, help="body acceleration along x (workload default 1e-6)")
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -404,6 +456,23 @@ def main():
                        "force accumulation on"}
         torch.cuda.empty_cache()
 
+    moving = None
+    if not args.no_moving:
+        m_steps = max(20, min(4 * args.steps, 400))
+        ms_m, l_m, cells_m = time_moving_body(m_steps, args.warmup, local, stream, dist)
+        if dist is not None:
+            t = torch.tensor([ms_m], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_m = float(t.item())
+        moving = {"workload": "oscillating sphere channel 192x96x96 D3Q19 TRT tau+=0.56 Lambda=3/16, r=10, "
+                              "y_c(t)=48+8 sin(2 pi t/2000), inlet u_x=0.03, FP32",
+                  "value": round(world * cells_m * m_steps / (ms_m * 1e-3) / 1e6, 1), "unit": UNIT,
+                  "ms_per_step": round(ms_m / m_steps, 4), "steps": m_steps,
+                  "launches_per_step": round(l_m / m_steps, 2),
+                  "path": "host poses -> lbm_update_body -> lbm_step(1): moving-body flags and links in the "
+                          "body's box, refill, face-aware step kernel"}
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline()
@@ -422,6 +491,8 @@ def main():
         }
         if secondary:
             line["fp16dev"] = secondary
+        if moving:
+            line["moving_body"] = moving
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
