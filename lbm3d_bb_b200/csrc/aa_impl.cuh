@@ -30,7 +30,6 @@
 #pragma once
 #include "lbm_internal.cuh"
 #include "lbm_kernels.h"
-#include "f32x2.cuh"
 
 #ifndef LBM_MINB_F32
 #define LBM_MINB_F32 4
@@ -38,17 +37,7 @@
 #ifndef LBM_MINB_F16
 #define LBM_MINB_F16 4
 #endif
-// launch shape of the packed-pair kernels: threads per block (a multiple of 64: rows of
-// 64 threads = 128 cells along x) and blocks per SM that the register budget must allow
-#ifndef LBM_PAIR2_THREADS
-#define LBM_PAIR2_THREADS 256
-#endif
-#ifndef LBM_PAIR2_MINB
-#define LBM_PAIR2_MINB 3
-#endif
-#ifndef LBM_QUAD2_MINB
-#define LBM_QUAD2_MINB 2
-#endif
+
 // blocks of BATCH_ITEM threads per SM that the batched kernel's register budget allows:
 // FP32 6 (80 registers; 2 % faster than 8 on the 512-domain sweep, 4 was slower), the
 // other storages 2 x MIN_BLOCKS
@@ -96,6 +85,34 @@ struct StF16 {
   }
   static __device__ __forceinline__ C ld_raw(const S* p) { return __half2float(*p); }
   static __device__ __forceinline__ void st_raw(S* p, C v) { *p = __float2half_rn(v); }
+};
+
+// Storage policy with explicit global-space population accesses (ld.global.cg and
+// st.global.cg): the batched kernel takes each domain's population pointer from a device
+// table, so the compiler cannot infer the address space and would emit generic loads and
+// stores.  Same values as the wrapped policy.
+template <class Base>
+struct GlobalSpace : Base {
+  using S = typename Base::S;
+  using C = typename Base::C;
+  static __device__ __forceinline__ C ld(const S* p, int d, C rho0) {
+    const S v = __ldcg(p);
+    return Base::ld(&v, d, rho0);
+  }
+  static __device__ __forceinline__ void st(S* p, C v, int d, C rho0) {
+    S t;
+    Base::st(&t, v, d, rho0);
+    __stcg(p, t);
+  }
+  static __device__ __forceinline__ C ld_raw(const S* p) {
+    const S v = __ldcg(p);
+    return Base::ld_raw(&v);
+  }
+  static __device__ __forceinline__ void st_raw(S* p, C v) {
+    S t;
+    Base::st_raw(&t, v);
+    __stcg(p, t);
+  }
 };
 
 // ---- collision ---------------------------------------------------------------------
@@ -949,21 +966,15 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_ker
 // to one add per access.  Measured on B200 (512^3 porous box): 11 % faster than the
 // joint pair kernel for FP16 storage; slower for FP32 and for the even phase, which
 // keep aa_pair_kernel.
+// The odd-phase update of the cell pair (x0, x0 + 1), x0 even, as described above; all 32
+// lanes of the warp take part (warp vote).
 template <class SP, bool TRT, int FORCE>
-__global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_split_kernel(const __grid_constant__ AAParams p,
-                                                                                typename SP::S* __restrict__ A,
-                                                                                const uint8_t* __restrict__ flags) {
+__device__ __forceinline__ void pair_split_cells(const AAParams& p, typename SP::S* __restrict__ A,
+                                                 const uint8_t* __restrict__ flags, const int x0, const int y,
+                                                 const int z, const bool inb, double* acc, bool& has_link) {
   using S = typename SP::S;
   using C = typename SP::C;
   const Grid& g = p.g;
-  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const bool inb = x0 < g.nx && y < g.ny;
-  clear_record(p.zero_next);
-  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  bool has_link = false;
   const long long i0 = inb ? node_index(g, x0, y, z) : 0;
   const bool coord_fast = inb && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
   uint32_t fl0 = F_SOLID, fl1 = F_SOLID;
@@ -1080,6 +1091,22 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_spl
     if (inb && !solid0) aa_general<SP, true, TRT, FORCE>(p, A, flags, x0, y, z, i0, (uint8_t)fl0, acc, &has_link);
     if (inb && !solid1) aa_general<SP, true, TRT, FORCE>(p, A, flags, x0 + 1, y, z, i0 + 1, (uint8_t)fl1, acc, &has_link);
   }
+}
+
+template <class SP, bool TRT, int FORCE>
+__global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_split_kernel(const __grid_constant__ AAParams p,
+                                                                                typename SP::S* __restrict__ A,
+                                                                                const uint8_t* __restrict__ flags) {
+  const Grid& g = p.g;
+  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = x0 < g.nx && y < g.ny;
+  clear_record(p.zero_next);
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  pair_split_cells<SP, TRT, FORCE>(p, A, flags, x0, y, z, inb, acc, has_link);
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
@@ -1192,197 +1219,26 @@ __global__ void __launch_bounds__(256, 2) aa_quad_even_kernel(const __grid_const
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
-// ---- packed-pair kernels: the collision of two cells per FP32x2 instruction -------------
-// Same data movement as aa_pair_kernel / aa_quad_even_kernel; the two x-adjacent cells of
-// a pair are the low and high lane of packed FP32 values (f32x2.cuh), so the moments and
-// the collision take one instruction per operation for both cells, and each direction's
-// result is stored as soon as it is known.
-template <class S>
-struct PairF2;
-template <>
-struct PairF2<float> {
-  static __device__ __forceinline__ F2 ld2(const float* p) {
-    return F2{*reinterpret_cast<const unsigned long long*>(p)};
-  }
-  static __device__ __forceinline__ float ld1(const float* p) { return *p; }
-  static __device__ __forceinline__ void st2(float* p, F2 v) { *reinterpret_cast<unsigned long long*>(p) = v.v; }
-  static __device__ __forceinline__ void st1(float* p, float v) { *p = v; }
-};
-template <>
-struct PairF2<__half> {
-  static __device__ __forceinline__ F2 ld2(const __half* p) { return f2_from_half2(*reinterpret_cast<const uint32_t*>(p)); }
-  static __device__ __forceinline__ float ld1(const __half* p) { return __half2float(*p); }
-  static __device__ __forceinline__ void st2(__half* p, F2 v) { *reinterpret_cast<uint32_t*>(p) = half2_from_f2(v); }
-  static __device__ __forceinline__ void st1(__half* p, float v) { *p = __float2half_rn(v); }
-};
-
-// Momentum exchange of the static link (x, o): c_o (f*_o + f*_o) with its torque about the
-// body centre; v is the stored value (a deviation when `dev`).
-__device__ __forceinline__ void link_force(const AAParams& p, const int x, const int y, const int z, const int o,
-                                           const float v, const bool dev, double* acc) {
-  const double t = 2.0 * (double)(dev ? v + wgt<float>(o) * (float)p.rho0 : v);
-  const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
-  const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
-  const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
-  const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
-  acc[0] += fx;
-  acc[1] += fy;
-  acc[2] += fz;
-  acc[3] += ry * fz - rz * fy;
-  acc[4] += rz * fx - rx * fz;
-  acc[5] += rx * fy - ry * fx;
-}
-
-__device__ __forceinline__ Coll2 coll2_of(const AAParams& p) {
-  return Coll2{(float)p.omega_p, (float)p.omega_m, (float)p.gacc[0], (float)p.gacc[1], (float)p.gacc[2]};
-}
-
-// Two cells per thread, packed collision (fully periodic boxes, nx a multiple of 128; FP32
-// storage, and FP16-deviation storage in the odd phase).
-template <class SP, bool ODD, bool TRT, int FORCE>
-__global__ void __launch_bounds__(LBM_PAIR2_THREADS, LBM_PAIR2_MINB) aa_pair2_kernel(const __grid_constant__ AAParams p,
-                                                                                 typename SP::S* __restrict__ A,
-                                                                                 const uint8_t* __restrict__ flags) {
-  using S = typename SP::S;
-  using IO = PairF2<S>;
-  constexpr bool DEV = SP::DEV;
-  const Grid& g = p.g;
-  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const bool inb = x0 < g.nx && y < g.ny;
-  clear_record(p.zero_next);
-  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  bool has_link = false;
-  const long long i0 = inb ? node_index(g, x0, y, z) : 0;
-  const bool coord_fast = inb && (!ODD || (y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1));
-  uint32_t fl0 = F_SOLID, fl1 = F_SOLID;
-  if (inb) {
-    const uint32_t fw = *reinterpret_cast<const unsigned short*>(flags + i0);
-    fl0 = fw & 0xFFu;
-    fl1 = fw >> 8;
-  }
-  const long long fix_lo = x0 == 0 ? (long long)g.nx : 0;            // cell 0 at x = 0
-  const long long fix_hi = x0 + 1 == g.nx - 1 ? (long long)g.nx : 0;  // cell 1 at x = nx - 1
-  // byte bases: the pair, and each cell with its periodic x wrap folded in
-  char* const Bi = reinterpret_cast<char*>(A + i0);
-  char* const B0 = reinterpret_cast<char*>(A + i0 + fix_lo);
-  char* const B1 = reinterpret_cast<char*>(A + i0 + 1 - fix_hi);
-  F2 f[Q];
-  if (coord_fast) {
-#pragma unroll
-    for (int d = 0; d < Q; d++) {
-      const long long o = p.offb_rd[d];
-      if (!ODD || cx(d) == 0)
-        f[d] = IO::ld2(reinterpret_cast<const S*>(Bi + o));
-      else if (cx(d) == 1)
-        f[d] = f2(IO::ld1(reinterpret_cast<const S*>(B0 + o)), IO::ld1(reinterpret_cast<const S*>(Bi + o) + 1));
-      else
-        f[d] = f2(IO::ld1(reinterpret_cast<const S*>(Bi + o)), IO::ld1(reinterpret_cast<const S*>(B1 + o)));
-    }
-  }
-  const bool solid0 = (fl0 & F_SOLID) != 0, solid1 = (fl1 & F_SOLID) != 0;
-  uint32_t bc0 = 0, bc1 = 0;
-  bool st0 = true, st1 = true;
-  if (!solid0 && (fl0 & F_NEAR)) {
-    const unsigned long long lw = p.links[i0];
-    bc0 = (uint32_t)(lw & 0x3FFFFu);
-    st0 = bc0 == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 && !(fl0 & F_SOLID_PREV);
-  }
-  if (!solid1 && (fl1 & F_NEAR)) {
-    const unsigned long long lw = p.links[i0 + 1];
-    bc1 = (uint32_t)(lw & 0x3FFFFu);
-    st1 = bc1 == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 && !(fl1 & F_SOLID_PREV);
-  }
-  const bool both_solid = solid0 && solid1;
-  const bool fast = coord_fast && st0 && st1;
-  if (__all_sync(0xffffffffu, both_solid || fast)) {
-    if (!both_solid) {
-      const float rho0 = (float)p.rho0;
-      if (ODD && (bc0 | bc1)) {  // bounce-back values are kept in the own slots
-#pragma unroll
-        for (int d = 0; d < 18; d++) {
-          if (!(((bc0 | bc1) >> d) & 1u)) continue;
-          const S* own = A + (long long)d * g.plane + i0;
-          const float a = ((bc0 >> d) & 1u) ? IO::ld1(own) : f2lo(f[d]);
-          const float b = ((bc1 >> d) & 1u) ? IO::ld1(own + 1) : f2hi(f[d]);
-          f[d] = f2(a, b);
-        }
-      }
-      if (solid0 || solid1) {  // a solid cell's lane runs on the rest state; its results are not stored
-#pragma unroll
-        for (int d = 0; d < Q; d++) f[d] = f2sel(f[d], f2s(DEV ? 0.0f : wgt<float>(d) * rho0), solid0, solid1);
-      }
-      const Coll2 k = coll2_of(p);
-      F2 rho, ux, uy, uz;
-      moments2<FORCE, DEV>(f, k, rho0, rho, ux, uy, uz);
-      if (!solid0 && !solid1 && !(bc0 | bc1)) {
-        // both cells fluid without links: branch-free stores
-        collide2<TRT, FORCE, DEV>(f, k, rho0, rho, ux, uy, uz, [&](const int j, const F2 v) {
-          if (!ODD) {  // own slot opp(j) of both cells: one word
-            IO::st2(reinterpret_cast<S*>(Bi + p.offb_wr[opp(j)]), v);
-            return;
-          }
-          const long long o = p.offb_wr[j];
-          if (cx(j) == 0) {
-            IO::st2(reinterpret_cast<S*>(Bi + o), v);
-          } else {
-            float a, b;
-            f2split(v, a, b);
-            if (cx(j) == 1) {
-              IO::st1(reinterpret_cast<S*>(Bi + o), a);
-              IO::st1(reinterpret_cast<S*>(B1 + o), b);
-            } else {
-              IO::st1(reinterpret_cast<S*>(B0 + o), a);
-              IO::st1(reinterpret_cast<S*>(Bi + o) + 1, b);
-            }
-          }
-        });
-      } else {
-        collide2<TRT, FORCE, DEV>(f, k, rho0, rho, ux, uy, uz, [&](const int j, const F2 v) {
-          float a, b;
-          f2split(v, a, b);
-          const int oj = opp(j);
-          if (p.compute_force && j < 18) {  // incoming opp(j) of a static link: momentum exchange
-            if ((bc0 >> oj) & 1u) link_force(p, x0, y, z, j, a, DEV, acc);
-            if ((bc1 >> oj) & 1u) link_force(p, x0 + 1, y, z, j, b, DEV, acc);
-          }
-          if (!ODD) {  // own slots; a solid cell's slots take 0 (nobody reads them)
-            IO::st2(A + (long long)oj * g.plane + i0, f2(solid0 ? 0.0f : a, solid1 ? 0.0f : b));
-            return;
-          }
-          const long long o = p.off_wr[j];
-          if (!solid0) {
-            long long ad = i0 + o + (cx(j) == -1 ? fix_lo : 0);
-            if (j < 18 && ((bc0 >> oj) & 1u)) ad = (long long)oj * g.plane + i0;
-            IO::st1(A + ad, a);
-          }
-          if (!solid1) {
-            long long ad = i0 + 1 + o - (cx(j) == 1 ? fix_hi : 0);
-            if (j < 18 && ((bc1 >> oj) & 1u)) ad = (long long)oj * g.plane + i0 + 1;
-            IO::st1(A + ad, b);
-          }
-        });
-        if (p.compute_force && (bc0 | bc1)) has_link = true;
-      }
-    }
-  } else {
-    if (inb && !solid0) aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x0, y, z, i0, (uint8_t)fl0, acc, &has_link);
-    if (inb && !solid1) aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x0 + 1, y, z, i0 + 1, (uint8_t)fl1, acc, &has_link);
-  }
-  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
-}
-
-// FP16-deviation even phase, four cells per thread (as aa_quad_even_kernel), the two
-// cell pairs of each 8-byte word collided as packed FP32 pairs: pair 0's results are
-// held as half2 words until pair 1's arrive, then both go out in one 8-byte store.
+// ---- quad kernel: odd phase, FP16-deviation storage ----------------------------------
+// One thread updates four x-adjacent cells (x0 .. x0+3, x0 a multiple of 4) and a warp 128
+// consecutive cells of one row.  Every direction moves as one aligned 8-byte word per
+// thread and direction (19 loads and 19 stores for four cells): for an x-shifted direction
+// the word of the same four positions is shifted by one element, the element that enters
+// from the neighbouring thread's word comes by warp shuffle, and only the warp's edge lanes
+// move one more element through memory (lane 0 and lane 31, with the periodic x wrap).
+// Every slot is still read and written by exactly one thread: an aligned word that a warp
+// covers only in part (its first element for pushes along +x, its last for pushes along -x)
+// gets the missing element from the neighbouring warp's edge lane.  Warps holding a solid,
+// near-boundary or uncovered cell, or a row next to a y/z wrap, run the split pair update on
+// their two cell pairs instead.
 template <bool TRT, int FORCE>
-__global__ void __launch_bounds__(256, LBM_QUAD2_MINB) aa_quad2_even_kernel(const __grid_constant__ AAParams p,
-                                                               __half* __restrict__ A,
-                                                               const uint8_t* __restrict__ flags) {
+__global__ void __launch_bounds__(256, 2) aa_quad_odd_kernel(const __grid_constant__ AAParams p,
+                                                             __half* __restrict__ A,
+                                                             const uint8_t* __restrict__ flags) {
   using SP = StF16;
+  using C = float;
   const Grid& g = p.g;
+  const int lane = threadIdx.x;  // blockDim.x == 32: one warp is one row segment
   const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
@@ -1394,75 +1250,106 @@ __global__ void __launch_bounds__(256, LBM_QUAD2_MINB) aa_quad2_even_kernel(cons
   const long long i0 = inb ? node_index(g, x0, y, z) : 0;
   uint32_t fw = 0x01010101u * F_SOLID;
   if (inb) fw = *reinterpret_cast<const uint32_t*>(flags + i0);
-  char* const Ai = reinterpret_cast<char*>(A + i0);
-  uint2 w[Q];
-  if (inb) {
+  // four fluid cells away from any solid (F_SOLID, F_SOLID_PREV, F_NEAR clear), not in a
+  // row next to the y/z wrap
+  const bool plain = inb && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1 && (fw & 0x07070707u) == 0u;
+  if (__all_sync(0xffffffffu, plain)) {
+    char* const Ai = reinterpret_cast<char*>(A + i0);
+    const long long wrap_lo = x0 == 0 ? 2LL * g.nx : 0;           // element x0 - 1 at x = nx - 1
+    const long long wrap_hi = x0 + 4 == g.nx ? 2LL * g.nx : 0;    // element x0 + 4 at x = 0
+    uint2 w[Q];
+    unsigned short edge[Q];
 #pragma unroll
-    for (int d = 0; d < Q; d++) w[d] = *reinterpret_cast<const uint2*>(Ai + p.offb_rd[d]);
-  }
-  uint32_t bc[4];
-  bool fast = true, any_fluid = false;
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const uint32_t fl = (fw >> (8 * k)) & 0xFFu;
-    bc[k] = 0;
-    if (!(fl & F_SOLID)) {
-      any_fluid = true;
-      if (fl & F_NEAR) {
-        const unsigned long long lw = p.links[i0 + k];
-        bc[k] = (uint32_t)(lw & 0x3FFFFu);
-        fast = fast && bc[k] == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 &&
-               !(fl & F_SOLID_PREV);
+    for (int d = 0; d < Q; d++) {
+      const long long o = p.offb_rd[d];
+      if (cx(d) == 0) {
+        w[d] = *reinterpret_cast<const uint2*>(Ai + o);
+      } else if (cx(d) == 1) {  // pull from x - 1: o addresses element x0 - 1 of the source row
+        w[d] = *reinterpret_cast<const uint2*>(Ai + o + 2);
+        if (lane == 0) edge[d] = *reinterpret_cast<const unsigned short*>(Ai + o + wrap_lo);
+      } else {  // pull from x + 1: o addresses element x0 + 1
+        w[d] = *reinterpret_cast<const uint2*>(Ai + o - 2);
+        if (lane == 31) edge[d] = *reinterpret_cast<const unsigned short*>(Ai + o + 6 - wrap_hi);
       }
     }
-  }
-  if (__all_sync(0xffffffffu, !any_fluid || fast)) {
-    if (any_fluid) {
-      const float rho0 = (float)p.rho0;
-      const Coll2 k = coll2_of(p);
-      const bool sol[4] = {((fw >> 0) & F_SOLID) != 0, ((fw >> 8) & F_SOLID) != 0, ((fw >> 16) & F_SOLID) != 0,
-                           ((fw >> 24) & F_SOLID) != 0};
-      uint32_t held[Q];  // pair 0's results, one half2 word per direction slot
+    // shift the x-pulled words by one element (element k = bits 16k .. 16k+15)
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const bool s0 = sol[2 * h], s1 = sol[2 * h + 1];
-        F2 f[Q];
+    for (int d = 0; d < Q; d++) {
+      if (cx(d) == 1) {  // [x0-1, x0, x0+1, x0+2]: the last element of the previous lane's word
+        const uint32_t up = __shfl_up_sync(0xffffffffu, w[d].y, 1) >> 16;
+        const uint32_t in = lane == 0 ? (uint32_t)edge[d] : up;
+        w[d] = make_uint2((w[d].x << 16) | in, __funnelshift_l(w[d].x, w[d].y, 16));
+      } else if (cx(d) == -1) {  // [x0+1 .. x0+4]: the first element of the next lane's word
+        const uint32_t dn = __shfl_down_sync(0xffffffffu, w[d].x, 1) & 0xFFFFu;
+        const uint32_t in = lane == 31 ? (uint32_t)edge[d] : dn;
+        w[d] = make_uint2(__funnelshift_r(w[d].x, w[d].y, 16), (w[d].y >> 16) | (in << 16));
+      }
+    }
+    // collide the cells in pairs (low and high half2 of each 32-bit word)
+    uint2 out[Q];
 #pragma unroll
-        for (int d = 0; d < Q; d++) f[d] = f2_from_half2(h ? w[d].y : w[d].x);
-        if (s0 || s1) {  // a solid cell's lane runs on the rest state; its slots take 0
+    for (int h = 0; h < 2; h++) {
+      C pa[Q], pb[Q];
+      {
+        C f[Q];
 #pragma unroll
-          for (int d = 0; d < Q; d++) f[d] = f2sel(f[d], f2s(0.0f), s0, s1);
+        for (int d = 0; d < Q; d++) {
+          const uint32_t u = h ? w[d].y : w[d].x;
+          f[d] = __low2float(*reinterpret_cast<const __half2*>(&u));
         }
-        F2 rho, ux, uy, uz;
-        moments2<FORCE, true>(f, k, rho0, rho, ux, uy, uz);
-        const uint32_t l0 = bc[2 * h], l1 = bc[2 * h + 1];
-        collide2<TRT, FORCE, true>(f, k, rho0, rho, ux, uy, uz, [&](const int j, F2 v) {
-          const int oj = opp(j);  // own slot oj takes the post-collision value of j
-          if ((s0 || s1) || (p.compute_force && (l0 | l1))) {
-            float a, b;
-            f2split(v, a, b);
-            if (p.compute_force && j < 18) {
-              if ((l0 >> oj) & 1u) link_force(p, x0 + 2 * h, y, z, j, a, true, acc);
-              if ((l1 >> oj) & 1u) link_force(p, x0 + 2 * h + 1, y, z, j, b, true, acc);
-            }
-            v = f2(s0 ? 0.0f : a, s1 ? 0.0f : b);
-          }
-          const uint32_t word = half2_from_f2(v);
-          if (h == 0)
-            held[oj] = word;
-          else
-            *reinterpret_cast<uint2*>(Ai + p.offb_wr[oj]) = make_uint2(held[oj], word);
-        });
-        if (p.compute_force && (l0 | l1)) has_link = true;
+        pair_cell<SP, true, TRT, FORCE>(p, f, pa);
+      }
+      {
+        C f[Q];
+#pragma unroll
+        for (int d = 0; d < Q; d++) {
+          const uint32_t u = h ? w[d].y : w[d].x;
+          f[d] = __high2float(*reinterpret_cast<const __half2*>(&u));
+        }
+        pair_cell<SP, true, TRT, FORCE>(p, f, pb);
+      }
+#pragma unroll
+      for (int j = 0; j < Q; j++) {  // push slot j takes the post-collision value of j
+        const __half2 v = __floats2half2_rn(pa[j], pb[j]);
+        const uint32_t u = *reinterpret_cast<const uint32_t*>(&v);
+        if (h)
+          out[j].y = u;
+        else
+          out[j].x = u;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+      const long long o = p.offb_wr[j];
+      if (cx(j) == 0) {
+        *reinterpret_cast<uint2*>(Ai + o) = out[j];
+      } else if (cx(j) == 1) {  // push to x + 1: o addresses element x0 + 1 of the target row
+        const uint32_t up = __shfl_up_sync(0xffffffffu, out[j].y, 1) >> 16;
+        if (lane != 0) {
+          *reinterpret_cast<uint2*>(Ai + o - 2) =
+              make_uint2((out[j].x << 16) | up, __funnelshift_l(out[j].x, out[j].y, 16));
+        } else {  // elements x0+1 .. x0+3; element x0 comes from the previous warp's lane 31
+          *reinterpret_cast<unsigned short*>(Ai + o) = (unsigned short)(out[j].x & 0xFFFFu);
+          *reinterpret_cast<uint32_t*>(Ai + o + 2) = __funnelshift_l(out[j].x, out[j].y, 16);
+        }
+        if (lane == 31)  // the fourth cell's value lands in the next warp's first word
+          *reinterpret_cast<unsigned short*>(Ai + o + 6 - wrap_hi) = (unsigned short)(out[j].y >> 16);
+      } else {  // push to x - 1: o addresses element x0 - 1
+        const uint32_t dn = __shfl_down_sync(0xffffffffu, out[j].x, 1) & 0xFFFFu;
+        if (lane != 31) {
+          *reinterpret_cast<uint2*>(Ai + o + 2) =
+              make_uint2(__funnelshift_r(out[j].x, out[j].y, 16), (out[j].y >> 16) | (dn << 16));
+        } else {  // elements x0 .. x0+2; element x0+3 comes from the next warp's lane 0
+          *reinterpret_cast<uint32_t*>(Ai + o + 2) = __funnelshift_r(out[j].x, out[j].y, 16);
+          *reinterpret_cast<unsigned short*>(Ai + o + 6) = (unsigned short)(out[j].y >> 16);
+        }
+        if (lane == 0)  // the first cell's value lands in the previous warp's last word
+          *reinterpret_cast<unsigned short*>(Ai + o + wrap_lo) = (unsigned short)(out[j].x & 0xFFFFu);
       }
     }
   } else {
-#pragma unroll 1
-    for (int k = 0; k < 4; k++) {
-      const uint32_t fl = (fw >> (8 * k)) & 0xFFu;
-      if (inb && !(fl & F_SOLID))
-        aa_general<SP, false, TRT, FORCE>(p, A, flags, x0 + k, y, z, i0 + k, (uint8_t)fl, acc, &has_link);
-    }
+    pair_split_cells<SP, TRT, FORCE>(p, A, flags, x0, y, z, inb, acc, has_link);
+    pair_split_cells<SP, TRT, FORCE>(p, A, flags, x0 + 2, y, z, inb, acc, has_link);
   }
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
@@ -1553,7 +1440,7 @@ __global__ void __launch_bounds__(BATCH_ITEM, LBM_BATCH_MINB(SP)) aa_batch_kerne
     int x, y;
     divmod_rcp(cell, g.nx, inv_nx, row, x);
     divmod_rcp(row, g.ny, inv_ny, z, y);
-    aa_direct<SP, ODD, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
+    aa_direct<GlobalSpace<SP>, ODD, TRT, FORCE, FACES>(sp, A, flags, x, y, (int)z, inb, acc, &has_link);
   }
   if (dom >= 0 && sp.compute_force) block_force_reduce(acc, has_link, rec + stripe);
 }
@@ -1869,23 +1756,13 @@ static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, 
   if constexpr (!FACES) {
     if (p.pair) {  // 64 x 4 threads, two cells each
       const dim3 pb(64, 4, 1), pg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 3) / 4), (unsigned)p.g.nz);
-      if constexpr (sizeof(typename SP::S) <= 4) {
-        if (p.packed) {  // collision on packed FP32 pairs
-          if constexpr (!ODD && SP::DEV) {
-            if (p.quad) {  // 32 x 8 threads, four cells each
-              const dim3 qb(32, 8, 1), qg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 7) / 8), (unsigned)p.g.nz);
-              aa_quad2_even_kernel<TRT, FORCE><<<qg, qb, 0, s>>>(p, (__half*)A, flags);
-              return cudaGetLastError();
-            }
-          }
-          constexpr int rows = LBM_PAIR2_THREADS / 64;
-          const dim3 b2(64, rows, 1), g2((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + rows - 1) / rows), (unsigned)p.g.nz);
-          aa_pair2_kernel<SP, ODD, TRT, FORCE><<<g2, b2, 0, s>>>(p, (typename SP::S*)A, flags);
-          return cudaGetLastError();
-        }
-      }
       if constexpr (ODD && SP::DEV) {
-        aa_pair_split_kernel<SP, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+        if (p.quad) {  // 32 x 8 threads, four cells each
+          const dim3 qb(32, 8, 1), qg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 7) / 8), (unsigned)p.g.nz);
+          aa_quad_odd_kernel<TRT, FORCE><<<qg, qb, 0, s>>>(p, (__half*)A, flags);
+        } else {
+          aa_pair_split_kernel<SP, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+        }
       } else if constexpr (!ODD && SP::DEV) {
         if (p.quad) {  // 32 x 8 threads, four cells each
           const dim3 qb(32, 8, 1), qg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 7) / 8), (unsigned)p.g.nz);

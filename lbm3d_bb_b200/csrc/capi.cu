@@ -77,7 +77,6 @@ struct lbm_ctx {
   int bx = 0, by = 0;
   bool pair = false;  // FP16 pair kernel (see aa_pair_kernel)
   bool quad = false;  // FP16-deviation even phase on aa_quad_even_kernel
-  bool packed = false;  // pair kernels collide on packed FP32 pairs (aa_pair2_kernel)
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -753,14 +752,10 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
                       (c->g.per[2] || halo_only(c));
     const bool wanted = env ? env[0] == '1' : cfg->storage != LBM_STORE_FP64;
     c->pair = fits && wanted;
-    // four cells per thread in the FP16-deviation even phase (4.5 % faster than the pair
-    // kernel on B200); LBM3D_QUAD=0 keeps the pair kernel
+    // four cells per thread in both FP16-deviation phases (aa_quad_even_kernel,
+    // aa_quad_odd_kernel); LBM3D_QUAD=0 keeps the pair kernels
     const char* q = std::getenv("LBM3D_QUAD");
     c->quad = c->pair && cfg->storage == LBM_STORE_FP16DEV && !(q && q[0] == '0');
-    // the collision of the two (four) cells of a thread on packed FP32 pairs, FP32 and
-    // FP16-deviation storage; LBM3D_PACKED=0 keeps the scalar pair kernels
-    const char* pk = std::getenv("LBM3D_PACKED");
-    c->packed = c->pair && cfg->storage != LBM_STORE_FP64 && !(pk && pk[0] == '0');
   }
   c->bytes += fl + ring_bytes + 64;
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);
@@ -1029,7 +1024,6 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
       p.zero_next = next;
       p.pair = c->pair ? 1 : 0;
       p.quad = c->pair && c->quad ? 1 : 0;
-      p.packed = c->pair && c->packed ? 1 : 0;
       if (c->tma) {
         if (c->tiles_dirty) {
           c->launches++;

@@ -42,7 +42,6 @@ struct AAParams {
   const unsigned long long* links;
   int pair;  // all axes periodic, nx % 128 == 0: two cells per thread (aa_pair_kernel)
   int quad;  // with pair, FP16-deviation even phase: four cells per thread (aa_quad_even_kernel)
-  int packed;  // with pair: the collision runs on packed FP32 pairs (aa_pair2_kernel, aa_quad2_even_kernel)
 };
 
 // Batched step over many independent config-mode domains (one launch per step).

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 def _case(cls, shape, solid_bc="IBB", **kw):
     nx, ny, nz = 64, 40, 3
-    U, Re = 0.06, 60.0
+    U, Re = 0.05, 30.0
     F = np.float32
     L = F(8.32) if shape == "cyl" else F(24.0)
     nu = F(U) * L / F(Re)
@@ -45,9 +45,10 @@ def _case(cls, shape, solid_bc="IBB", **kw):
 
 
 def _pose(shape, n):
-    """Heave (and, for the airfoil, pitch about 8 degrees) at t = n-1 and n-1/2."""
+    """Heave (and, for the airfoil, pitch about 8 degrees) at t = n-1 and n-1/2; the body
+    moves at most 0.03 lattice units per step."""
     F = np.float32
-    A, w = 1.3, 2.0 * math.pi / 40.0
+    A, w = 1.3, 2.0 * math.pi / 300.0
     yc0 = 20.3 if shape == "cyl" else 20.2
     xc = 20.5 if shape == "cyl" else 24.0
 

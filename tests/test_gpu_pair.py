@@ -86,11 +86,13 @@ def test_pair_kernel_vs_oracle(gpu, oracle_lib, storage):
     g.check_finite()
 
 
-@pytest.mark.parametrize("steps", [6, 7])
+@pytest.mark.parametrize("steps,nx", [(6, 128), (7, 128), (11, 256)])
 @pytest.mark.parametrize("collision", ["BGK", "TRT"])
-def test_quad_even_kernel_matches_pair_kernel(gpu, steps, collision):
-    """FP16-deviation even phase with four cells per thread (LBM3D_QUAD, default on)
-    against the pair kernel: same populations to storage rounding, same force history."""
+def test_quad_kernels_match_pair_kernels(gpu, steps, nx, collision):
+    """FP16-deviation with four cells per thread in both phases (LBM3D_QUAD, default on:
+    aa_quad_even_kernel, and aa_quad_odd_kernel with its word shifts, warp shuffles and
+    edge-lane elements, one or two warps per row) against the pair kernels: same
+    populations to storage rounding, same force history."""
     kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
     var = "LBM3D_QUAD"
 
@@ -99,7 +101,7 @@ def test_quad_even_kernel_matches_pair_kernel(gpu, steps, collision):
         os.environ[var] = "1" if quad else "0"
         try:
             rng = np.random.default_rng(11)
-            nx, ny, nz = 128, 20, 16
+            ny, nz = 20, 16
             xyzr = np.concatenate([rng.uniform(0, [nx, ny, nz], (6, 3)), rng.uniform(2.0, 4.5, (6, 1))], axis=1)
             d = Domain(nx, ny, nz, collision=collision, storage="fp16dev", faces=cases.PERIODIC, omega_p=1.0 / 0.6,
                        accel=(1e-5, 0.0, 0.0), compute_force=True, **kw)
