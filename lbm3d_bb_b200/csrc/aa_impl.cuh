@@ -818,21 +818,15 @@ __device__ __forceinline__ void pair_links(const AAParams& p, const int x, const
   }
 }
 
+// The update of the cell pair (x0, x0 + 1), x0 even, as described above; all 32 lanes of the
+// warp take part (warp vote).
 template <class SP, bool ODD, bool TRT, int FORCE>
-__global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_kernel(const __grid_constant__ AAParams p,
-                                                                                typename SP::S* __restrict__ A,
-                                                                                const uint8_t* __restrict__ flags) {
+__device__ __forceinline__ void pair_cells(const AAParams& p, typename SP::S* __restrict__ A,
+                                           const uint8_t* __restrict__ flags, const int x0, const int y, const int z,
+                                           const bool inb, double* acc, bool& has_link) {
   using S = typename SP::S;
   using C = typename SP::C;
   const Grid& g = p.g;
-  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const bool inb = x0 < g.nx && y < g.ny;
-  clear_record(p.zero_next);
-  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
-  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  bool has_link = false;
   const long long i0 = inb ? node_index(g, x0, y, z) : 0;
   const bool coord_fast = inb && (!ODD || (y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1));
   uint32_t fl0 = F_SOLID, fl1 = F_SOLID;
@@ -955,6 +949,119 @@ __global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_ker
   } else {
     if (inb && !solid0) aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x0, y, z, i0, (uint8_t)fl0, acc, &has_link);
     if (inb && !solid1) aa_general<SP, ODD, TRT, FORCE>(p, A, flags, x0 + 1, y, z, i0 + 1, (uint8_t)fl1, acc, &has_link);
+  }
+}
+
+template <class SP, bool ODD, bool TRT, int FORCE>
+__global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_kernel(const __grid_constant__ AAParams p,
+                                                                                typename SP::S* __restrict__ A,
+                                                                                const uint8_t* __restrict__ flags) {
+  const Grid& g = p.g;
+  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = x0 < g.nx && y < g.ny;
+  clear_record(p.zero_next);
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  pair_cells<SP, ODD, TRT, FORCE>(p, A, flags, x0, y, z, inb, acc, has_link);
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
+}
+
+// Odd phase of the pair kernel with every direction moved as one aligned two-element word
+// per thread (FP32 storage): an x-shifted direction takes the word of the thread's own two
+// positions, the element that enters from the neighbouring thread comes by warp shuffle,
+// and only the warp's edge lanes (0 and 31) move one more element through memory, with the
+// periodic x wrap.  Each slot is read and written by exactly one thread: an aligned word a
+// warp covers only in part gets its missing element from the neighbouring warp's edge lane.
+// Warps holding a solid, near-boundary or uncovered cell, or a row next to a y/z wrap, run
+// the pair update above.
+template <class SP, bool TRT, int FORCE>
+__global__ void __launch_bounds__(256, (SP::MIN_BLOCKS > 2 ? 3 : 1)) aa_pair_odd_kernel(const __grid_constant__ AAParams p,
+                                                                                    typename SP::S* __restrict__ A,
+                                                                                    const uint8_t* __restrict__ flags) {
+  using S = typename SP::S;
+  using C = typename SP::C;
+  static_assert(sizeof(S) == 4 && !SP::DEV, "FP32 storage");
+  const Grid& g = p.g;
+  const int lane = threadIdx.x & 31;  // blockDim.x is a multiple of 32: a warp is 64 cells of a row
+  const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = x0 < g.nx && y < g.ny;
+  clear_record(p.zero_next);
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  const long long i0 = inb ? node_index(g, x0, y, z) : 0;
+  uint32_t fw = 0x0101u * F_SOLID;
+  if (inb) fw = *reinterpret_cast<const unsigned short*>(flags + i0);
+  // two fluid cells away from any solid (F_SOLID, F_SOLID_PREV, F_NEAR clear), not in a row
+  // next to the y/z wrap
+  const bool plain = inb && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1 && (fw & 0x0707u) == 0u;
+  if (__all_sync(0xffffffffu, plain)) {
+    constexpr long long E = sizeof(S);
+    char* const Ai = reinterpret_cast<char*>(A + i0);
+    const long long wrap_lo = x0 == 0 ? E * g.nx : 0;          // element x0 - 1 at x = nx - 1
+    const long long wrap_hi = x0 + 2 == g.nx ? E * g.nx : 0;   // element x0 + 2 at x = 0
+    C f0[Q], f1[Q];
+    C edge[Q];
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      const long long o = p.offb_rd[d];
+      if (cx(d) == 0) {
+        const float2 v = *reinterpret_cast<const float2*>(Ai + o);
+        f0[d] = v.x;
+        f1[d] = v.y;
+      } else if (cx(d) == 1) {  // pull from x - 1: o addresses element x0 - 1 of the source row
+        const float2 v = *reinterpret_cast<const float2*>(Ai + o + E);
+        f0[d] = v.y;  // replaced by the previous lane's second element below
+        f1[d] = v.x;
+        if (lane == 0) edge[d] = *reinterpret_cast<const S*>(Ai + o + wrap_lo);
+      } else {  // pull from x + 1: o addresses element x0 + 1
+        const float2 v = *reinterpret_cast<const float2*>(Ai + o - E);
+        f0[d] = v.y;
+        f1[d] = v.x;  // replaced by the next lane's first element below
+        if (lane == 31) edge[d] = *reinterpret_cast<const S*>(Ai + o + E - wrap_hi);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      if (cx(d) == 1) {
+        const C up = __shfl_up_sync(0xffffffffu, f0[d], 1);
+        f0[d] = lane == 0 ? edge[d] : up;
+      } else if (cx(d) == -1) {
+        const C dn = __shfl_down_sync(0xffffffffu, f1[d], 1);
+        f1[d] = lane == 31 ? edge[d] : dn;
+      }
+    }
+    C p0[Q], p1[Q];
+    pair_cell<SP, true, TRT, FORCE>(p, f0, p0);
+    pair_cell<SP, true, TRT, FORCE>(p, f1, p1);
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+      const long long o = p.offb_wr[j];
+      if (cx(j) == 0) {
+        *reinterpret_cast<float2*>(Ai + o) = make_float2(p0[j], p1[j]);
+      } else if (cx(j) == 1) {  // push to x + 1: o addresses element x0 + 1 of the target row
+        const C up = __shfl_up_sync(0xffffffffu, p1[j], 1);
+        if (lane != 0)
+          *reinterpret_cast<float2*>(Ai + o - E) = make_float2(up, p0[j]);
+        else  // element x0 comes from the previous warp's lane 31
+          *reinterpret_cast<S*>(Ai + o) = p0[j];
+        if (lane == 31) *reinterpret_cast<S*>(Ai + o + E - wrap_hi) = p1[j];
+      } else {  // push to x - 1: o addresses element x0 - 1
+        const C dn = __shfl_down_sync(0xffffffffu, p0[j], 1);
+        if (lane != 31)
+          *reinterpret_cast<float2*>(Ai + o + E) = make_float2(p1[j], dn);
+        else  // element x0 + 1 comes from the next warp's lane 0
+          *reinterpret_cast<S*>(Ai + o + E) = p1[j];
+        if (lane == 0) *reinterpret_cast<S*>(Ai + o + wrap_lo) = p0[j];
+      }
+    }
+  } else {
+    pair_cells<SP, true, TRT, FORCE>(p, A, flags, x0, y, z, inb, acc, has_link);
   }
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
@@ -1770,6 +1877,11 @@ static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, 
         } else {
           aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
         }
+      } else if constexpr (ODD && sizeof(typename SP::S) == 4) {
+        if (p.xshuffle)
+          aa_pair_odd_kernel<SP, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
+        else
+          aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
       } else {
         aa_pair_kernel<SP, ODD, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
       }

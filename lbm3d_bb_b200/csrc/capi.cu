@@ -76,7 +76,8 @@ struct lbm_ctx {
   // launch shape
   int bx = 0, by = 0;
   bool pair = false;  // FP16 pair kernel (see aa_pair_kernel)
-  bool quad = false;  // FP16-deviation even phase on aa_quad_even_kernel
+  bool quad = false;  // FP16-deviation on the four-cell kernels
+  bool xshuffle = false;  // FP32 odd phase on aa_pair_odd_kernel
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -756,6 +757,10 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     // aa_quad_odd_kernel); LBM3D_QUAD=0 keeps the pair kernels
     const char* q = std::getenv("LBM3D_QUAD");
     c->quad = c->pair && cfg->storage == LBM_STORE_FP16DEV && !(q && q[0] == '0');
+    // FP32 odd phase with the x-shifted directions moved as shuffled two-element words;
+    // LBM3D_XSHUFFLE=0 keeps the pair kernel
+    const char* xs = std::getenv("LBM3D_XSHUFFLE");
+    c->xshuffle = c->pair && cfg->storage == LBM_STORE_FP32 && !(xs && xs[0] == '0');
   }
   c->bytes += fl + ring_bytes + 64;
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);
@@ -1024,6 +1029,7 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
       p.zero_next = next;
       p.pair = c->pair ? 1 : 0;
       p.quad = c->pair && c->quad ? 1 : 0;
+      p.xshuffle = c->pair && c->xshuffle ? 1 : 0;
       if (c->tma) {
         if (c->tiles_dirty) {
           c->launches++;

@@ -151,3 +151,41 @@ def test_x_only_force_matches_general_force(gpu, collision):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("nx,steps", [(128, 9), (256, 10)])
+@pytest.mark.parametrize("collision", ["BGK", "TRT"])
+def test_fp32_shuffled_odd_phase_matches_pair_kernel(gpu, nx, steps, collision):
+    """FP32 odd phase with the x-shifted directions moved as shuffled two-element words
+    (LBM3D_XSHUFFLE, default on: aa_pair_odd_kernel, one or two warps per row, warps with
+    solids or links on the pair update) against the pair kernel: the same arithmetic on
+    the same values, so the same bits."""
+    kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
+    var = "LBM3D_XSHUFFLE"
+
+    def run(on):
+        old = os.environ.get(var)
+        os.environ[var] = "1" if on else "0"
+        try:
+            rng = np.random.default_rng(13)
+            ny, nz = 16, 12
+            xyzr = np.concatenate([rng.uniform(0, [nx, ny, nz], (6, 3)), rng.uniform(2.0, 4.5, (6, 1))], axis=1)
+            d = Domain(nx, ny, nz, collision=collision, storage="fp32", faces=cases.PERIODIC, omega_p=1.0 / 0.6,
+                       accel=(1e-5, 0.0, 0.0), compute_force=True, **kw)
+            d.add_spheres(xyzr)
+            d.init_equilibrium()
+            d.step(steps)
+            return d
+        finally:
+            if old is None:
+                del os.environ[var]
+            else:
+                os.environ[var] = old
+
+    a, b = run(True), run(False)
+    try:
+        assert np.array_equal(a.populations(np.float32), b.populations(np.float32))
+        assert np.array_equal(a.force_history(1, steps), b.force_history(1, steps))
+    finally:
+        a.close()
+        b.close()
