@@ -1326,6 +1326,122 @@ __global__ void __launch_bounds__(256, 2) aa_quad_even_kernel(const __grid_const
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
+// ---- octo kernel: even phase, FP16-deviation storage -----------------------------------
+// Eight x-adjacent cells per thread (x0 a multiple of 8): one aligned 16-byte word per
+// direction, 19 loads and 19 stores of 128 bits for eight cells.  The cells collide in pairs
+// (the four half2 lanes of the words); each pair's results replace that pair's lane of the
+// words at once (its inputs are consumed by then), so the words hold inputs and outputs
+// without a second set of registers.
+__device__ __forceinline__ uint32_t u4get(const uint4& v, const int k) {
+  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void u4set(uint4& v, const int k, const uint32_t u) {
+  if (k == 0) v.x = u;
+  else if (k == 1) v.y = u;
+  else if (k == 2) v.z = u;
+  else v.w = u;
+}
+
+template <bool TRT, int FORCE>
+__global__ void __launch_bounds__(128, 3) aa_octo_even_kernel(const __grid_constant__ AAParams p,
+                                                              __half* __restrict__ A,
+                                                              const uint8_t* __restrict__ flags) {
+  using SP = StF16;
+  using C = float;
+  const Grid& g = p.g;
+  const int x0 = 8 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool inb = x0 < g.nx && y < g.ny;
+  clear_record(p.zero_next);
+  if (ghost_plane(p, z)) return;  // whole block in a ghost plane
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  bool has_link = false;
+  const long long i0 = inb ? node_index(g, x0, y, z) : 0;
+  uint2 fw = make_uint2(0x01010101u * F_SOLID, 0x01010101u * F_SOLID);
+  if (inb) fw = *reinterpret_cast<const uint2*>(flags + i0);
+  char* const Ai = reinterpret_cast<char*>(A + i0);
+  uint4 w[Q];
+  if (inb) {
+#pragma unroll
+    for (int d = 0; d < Q; d++) w[d] = *reinterpret_cast<const uint4*>(Ai + p.offb_rd[d]);
+  }
+  bool fast = true, any_fluid = false;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const uint32_t fl = ((k < 4 ? fw.x : fw.y) >> (8 * (k & 3))) & 0xFFu;
+    if (!(fl & F_SOLID)) {
+      any_fluid = true;
+      if (fl & F_NEAR) {
+        const unsigned long long lw = p.links[i0 + k];
+        const uint32_t b = (uint32_t)(lw & 0x3FFFFu);
+        fast = fast && b == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0 && !(fl & F_SOLID_PREV);
+      }
+    }
+  }
+  if (__all_sync(0xffffffffu, !any_fluid || fast)) {
+    if (any_fluid) {
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        const int ka = 2 * h, kb = 2 * h + 1;
+        const uint32_t fla = ((h < 2 ? fw.x : fw.y) >> (16 * (h & 1))) & 0xFFu;
+        const uint32_t flb = ((h < 2 ? fw.x : fw.y) >> (16 * (h & 1) + 8)) & 0xFFu;
+        C pa[Q], pb[Q];
+        {
+          C f[Q];
+#pragma unroll
+          for (int d = 0; d < Q; d++) {
+            const uint32_t u = u4get(w[d], h);
+            f[d] = __low2float(*reinterpret_cast<const __half2*>(&u));
+          }
+          if (!(fla & F_SOLID)) {
+            pair_cell<SP, false, TRT, FORCE>(p, f, pa);
+          } else {
+#pragma unroll
+            for (int d = 0; d < Q; d++) pa[d] = C(0);
+          }
+        }
+        {
+          C f[Q];
+#pragma unroll
+          for (int d = 0; d < Q; d++) {
+            const uint32_t u = u4get(w[d], h);
+            f[d] = __high2float(*reinterpret_cast<const __half2*>(&u));
+          }
+          if (!(flb & F_SOLID)) {
+            pair_cell<SP, false, TRT, FORCE>(p, f, pb);
+          } else {
+#pragma unroll
+            for (int d = 0; d < Q; d++) pb[d] = C(0);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < Q; j++) {  // own slot j takes the post-collision value of opp(j)
+          const __half2 v = __floats2half2_rn(pa[opp(j)], pb[opp(j)]);
+          u4set(w[j], h, *reinterpret_cast<const uint32_t*>(&v));
+        }
+        if (p.compute_force && ((fla | flb) & F_NEAR)) {
+          const unsigned long long la = (fla & F_NEAR) ? p.links[i0 + ka] : 0ull;
+          const unsigned long long lb = (flb & F_NEAR) ? p.links[i0 + kb] : 0ull;
+          pair_links<SP>(p, x0 + ka, y, z, (uint32_t)(la & 0x3FFFFu), pa, acc);
+          pair_links<SP>(p, x0 + kb, y, z, (uint32_t)(lb & 0x3FFFFu), pb, acc);
+          has_link = has_link || ((la | lb) & 0x3FFFFu) != 0;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < Q; j++) *reinterpret_cast<uint4*>(Ai + p.offb_wr[j]) = w[j];
+    }
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < 8; k++) {
+      const uint32_t fl = ((k < 4 ? fw.x : fw.y) >> (8 * (k & 3))) & 0xFFu;
+      if (inb && !(fl & F_SOLID))
+        aa_general<SP, false, TRT, FORCE>(p, A, flags, x0 + k, y, z, i0 + k, (uint8_t)fl, acc, &has_link);
+    }
+  }
+  if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
+}
+
 // ---- quad kernel: odd phase, FP16-deviation storage ----------------------------------
 // One thread updates four x-adjacent cells (x0 .. x0+3, x0 a multiple of 4) and a warp 128
 // consecutive cells of one row.  Every direction moves as one aligned 8-byte word per
@@ -1871,7 +1987,10 @@ static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, 
           aa_pair_split_kernel<SP, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);
         }
       } else if constexpr (!ODD && SP::DEV) {
-        if (p.quad) {  // 32 x 8 threads, four cells each
+        if (p.quad == 2) {  // 32 x 4 threads, eight cells each (nx a multiple of 256)
+          const dim3 ob(32, 4, 1), og((unsigned)(p.g.nx / 256), (unsigned)((p.g.ny + 3) / 4), (unsigned)p.g.nz);
+          aa_octo_even_kernel<TRT, FORCE><<<og, ob, 0, s>>>(p, (__half*)A, flags);
+        } else if (p.quad) {  // 32 x 8 threads, four cells each
           const dim3 qb(32, 8, 1), qg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 7) / 8), (unsigned)p.g.nz);
           aa_quad_even_kernel<TRT, FORCE><<<qg, qb, 0, s>>>(p, (__half*)A, flags);
         } else {

@@ -78,6 +78,7 @@ struct lbm_ctx {
   bool pair = false;  // FP16 pair kernel (see aa_pair_kernel)
   bool quad = false;  // FP16-deviation on the four-cell kernels
   bool xshuffle = false;  // FP32 odd phase on aa_pair_odd_kernel
+  bool octo = false;  // FP16-deviation even phase on aa_octo_even_kernel
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -757,6 +758,10 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     // aa_quad_odd_kernel); LBM3D_QUAD=0 keeps the pair kernels
     const char* q = std::getenv("LBM3D_QUAD");
     c->quad = c->pair && cfg->storage == LBM_STORE_FP16DEV && !(q && q[0] == '0');
+    // eight cells per thread in the FP16-deviation even phase (16-byte words; nx a multiple
+    // of 256): LBM3D_OCTO=1
+    const char* oc = std::getenv("LBM3D_OCTO");
+    c->octo = c->quad && cfg->nx % 256 == 0 && (oc && oc[0] == '1');
     // FP32 odd phase with the x-shifted directions moved as shuffled two-element words;
     // LBM3D_XSHUFFLE=0 keeps the pair kernel
     const char* xs = std::getenv("LBM3D_XSHUFFLE");
@@ -1028,7 +1033,7 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
       p.force = slot;
       p.zero_next = next;
       p.pair = c->pair ? 1 : 0;
-      p.quad = c->pair && c->quad ? 1 : 0;
+      p.quad = c->pair && c->quad ? (c->octo && !c->swapped ? 2 : 1) : 0;
       p.xshuffle = c->pair && c->xshuffle ? 1 : 0;
       if (c->tma) {
         if (c->tiles_dirty) {

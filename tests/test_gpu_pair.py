@@ -189,3 +189,30 @@ def test_fp32_shuffled_odd_phase_matches_pair_kernel(gpu, nx, steps, collision):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("steps", [4, 7])
+def test_octo_even_kernel_matches_quad_kernel(gpu, steps):
+    """FP16-deviation even phase with eight cells per thread and 16-byte words
+    (LBM3D_OCTO=1, nx a multiple of 256) against the four-cell kernel: the same per-cell
+    arithmetic, so the same bits; the porous box mixes plain and boundary warps."""
+    var = "LBM3D_OCTO"
+
+    def run(on):
+        old = os.environ.get(var)
+        os.environ[var] = "1" if on else "0"
+        try:
+            return _porous(Domain, steps, "fp16dev", nx=256, ny=12, nz=10, seed=17)
+        finally:
+            if old is None:
+                del os.environ[var]
+            else:
+                os.environ[var] = old
+
+    a, b = run(True), run(False)
+    try:
+        assert np.array_equal(a.populations(np.float32), b.populations(np.float32))
+        assert np.array_equal(a.force_history(1, steps), b.force_history(1, steps))
+    finally:
+        a.close()
+        b.close()
