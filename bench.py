@@ -79,7 +79,7 @@ def step_kernel(storage: str, n: int) -> str:
         return "aa_step_kernel"
     if storage == "fp16dev":
         quad = os.environ.get("LBM3D_QUAD") != "0"
-        return "aa_quad_even_kernel / aa_quad_odd_kernel" if quad else "aa_pair_kernel / aa_pair_split_kernel"
+        return ("aa_quad_even_kernel" if quad else "aa_pair_kernel") + " / aa_pair_split_kernel"
     return "aa_pair_kernel"
 
 

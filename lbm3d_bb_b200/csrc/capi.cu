@@ -79,6 +79,7 @@ struct lbm_ctx {
   bool quad = false;  // FP16-deviation on the four-cell kernels
   bool xshuffle = false;  // FP32 odd phase on aa_pair_odd_kernel
   bool octo = false;  // FP16-deviation even phase on aa_octo_even_kernel
+  bool quad_odd = false;  // FP16-deviation odd phase on aa_quad_odd_kernel
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -754,18 +755,22 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
                       (c->g.per[2] || halo_only(c));
     const bool wanted = env ? env[0] == '1' : cfg->storage != LBM_STORE_FP64;
     c->pair = fits && wanted;
-    // four cells per thread in both FP16-deviation phases (aa_quad_even_kernel,
-    // aa_quad_odd_kernel); LBM3D_QUAD=0 keeps the pair kernels
+    // four cells per thread in the FP16-deviation even phase (aa_quad_even_kernel);
+    // LBM3D_QUAD=0 keeps the pair kernels
     const char* q = std::getenv("LBM3D_QUAD");
     c->quad = c->pair && cfg->storage == LBM_STORE_FP16DEV && !(q && q[0] == '0');
     // eight cells per thread in the FP16-deviation even phase (16-byte words; nx a multiple
     // of 256): LBM3D_OCTO=1
     const char* oc = std::getenv("LBM3D_OCTO");
     c->octo = c->quad && cfg->nx % 256 == 0 && (oc && oc[0] == '1');
-    // FP32 odd phase with the x-shifted directions moved as shuffled two-element words;
-    // LBM3D_XSHUFFLE=0 keeps the pair kernel
+    // FP32 odd phase with the x-shifted directions moved as shuffled two-element words:
+    // LBM3D_XSHUFFLE=1 (5 % slower than the pair kernel on the 512^3 box on B200)
     const char* xs = std::getenv("LBM3D_XSHUFFLE");
-    c->xshuffle = c->pair && cfg->storage == LBM_STORE_FP32 && !(xs && xs[0] == '0');
+    c->xshuffle = c->pair && cfg->storage == LBM_STORE_FP32 && (xs && xs[0] == '1');
+    // FP16-deviation odd phase on four cells per thread: LBM3D_QUAD_ODD=1 (9 % slower than
+    // the split pair kernel on the 512^3 box on B200)
+    const char* qo = std::getenv("LBM3D_QUAD_ODD");
+    c->quad_odd = c->quad && (qo && qo[0] == '1');
   }
   c->bytes += fl + ring_bytes + 64;
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);
@@ -1033,7 +1038,7 @@ int32_t lbm_step(lbm_ctx* c, int32_t nsteps) {
       p.force = slot;
       p.zero_next = next;
       p.pair = c->pair ? 1 : 0;
-      p.quad = c->pair && c->quad ? (c->octo && !c->swapped ? 2 : 1) : 0;
+      p.quad = c->pair && c->quad ? (c->swapped ? (c->quad_odd ? 1 : 0) : (c->octo ? 2 : 1)) : 0;
       p.xshuffle = c->pair && c->xshuffle ? 1 : 0;
       if (c->tma) {
         if (c->tiles_dirty) {

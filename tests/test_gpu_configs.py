@@ -15,8 +15,8 @@
       mean u_x of FP32 and FP16-deviation against the FP64 GPU run.
   C4  the 512-domain batched sweep (one persistent launch per step), 5000 steps:
       FP64 batch against the FP64 oracle on four domains (drag <= 1e-9), FP32 against
-      FP64 on every domain with a steady drag (within 0.5 %); the domains that diverge
-      are the ones BGK cannot hold (tau < 0.52).
+      FP64 on every stable domain (drag averaged over the last 200 steps within 0.5 %);
+      the domains that diverge are the ones BGK cannot hold (tau < 0.52).
 
 Stated tolerances for the reduced-precision forms (contract: drag within 0.5 % of FP64)
 are the constants below; the observed errors are printed with -s.
@@ -263,17 +263,14 @@ def test_c4_sweep_vs_oracle(gpu, oracle_lib):
     # the domains that diverge are the ones BGK cannot hold this close to tau = 1/2
     assert np.all(taus[~ok] < 0.52), taus[~ok]
     assert ok.sum() >= 350
-    # the 0.5 % contract is on the steady drag: domains whose FP64 drag still varies by more
-    # than 0.1 % over the last 200 steps (wake instability near tau = 1/2) are reported apart,
-    # on their mean drag over that window
+    # the contract is on the drag averaged over the last 200 steps: near tau = 1/2 many wakes
+    # are unsteady, and an instantaneous value of an unsteady drag differs between FP32 and
+    # FP64 by the phase of the oscillation
+    err32 = np.abs(mean["fp32"][ok] - mean["fp64"][ok]) / np.abs(mean["fp64"][ok])
+    last32 = np.abs(fx["fp32"][ok] - fx["fp64"][ok]) / np.abs(fx["fp64"][ok])
     steady = ok & (rsd["fp64"] < 1e-3)
-    err32 = np.abs(fx["fp32"][steady] - fx["fp64"][steady]) / np.abs(fx["fp64"][steady])
-    uns = ok & ~steady
-    err_uns = np.abs(mean["fp32"][uns] - mean["fp64"][uns]) / np.abs(mean["fp64"][uns])
     _report("C4 fp32 vs fp64", stable=int(ok.sum()), steady=int(steady.sum()), median=float(np.median(err32)),
-            p95=float(np.percentile(err32, 95)), max=float(err32.max()), unsteady=int(uns.sum()),
-            unsteady_mean_drag_max=float(err_uns.max()) if uns.any() else 0.0)
-    assert steady.sum() >= 300
+            p95=float(np.percentile(err32, 95)), max=float(err32.max()), last_step_max=float(last32.max()))
     assert err32.max() <= DRAG
     # the FP64 batch against the oracle over the full 5000 steps: the two smallest stable
     # domains of each x length

@@ -90,15 +90,16 @@ def test_pair_kernel_vs_oracle(gpu, oracle_lib, storage):
 @pytest.mark.parametrize("collision", ["BGK", "TRT"])
 def test_quad_kernels_match_pair_kernels(gpu, steps, nx, collision):
     """FP16-deviation with four cells per thread in both phases (LBM3D_QUAD, default on:
-    aa_quad_even_kernel, and aa_quad_odd_kernel with its word shifts, warp shuffles and
-    edge-lane elements, one or two warps per row) against the pair kernels: same
-    populations to storage rounding, same force history."""
+    aa_quad_even_kernel; with LBM3D_QUAD_ODD=1 also aa_quad_odd_kernel with its word shifts,
+    warp shuffles and edge-lane elements, one or two warps per row) against the pair
+    kernels: same populations to storage rounding, same force history."""
     kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
     var = "LBM3D_QUAD"
 
     def run(quad):
         old = os.environ.get(var)
         os.environ[var] = "1" if quad else "0"
+        os.environ["LBM3D_QUAD_ODD"] = "1" if quad else "0"
         try:
             rng = np.random.default_rng(11)
             ny, nz = 20, 16
@@ -110,6 +111,7 @@ def test_quad_kernels_match_pair_kernels(gpu, steps, nx, collision):
             d.step(steps)
             return d
         finally:
+            del os.environ["LBM3D_QUAD_ODD"]
             if old is None:
                 del os.environ[var]
             else:
@@ -157,9 +159,9 @@ def test_x_only_force_matches_general_force(gpu, collision):
 @pytest.mark.parametrize("collision", ["BGK", "TRT"])
 def test_fp32_shuffled_odd_phase_matches_pair_kernel(gpu, nx, steps, collision):
     """FP32 odd phase with the x-shifted directions moved as shuffled two-element words
-    (LBM3D_XSHUFFLE, default on: aa_pair_odd_kernel, one or two warps per row, warps with
-    solids or links on the pair update) against the pair kernel: the same arithmetic on
-    the same values, so the same bits."""
+    (LBM3D_XSHUFFLE=1: aa_pair_odd_kernel, one or two warps per row, warps with solids or
+    links on the pair update) against the pair kernel: the same arithmetic on the same
+    values, so the same bits."""
     kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
     var = "LBM3D_XSHUFFLE"
 
@@ -185,7 +187,10 @@ def test_fp32_shuffled_odd_phase_matches_pair_kernel(gpu, nx, steps, collision):
     a, b = run(True), run(False)
     try:
         assert np.array_equal(a.populations(np.float32), b.populations(np.float32))
-        assert np.array_equal(a.force_history(1, steps), b.force_history(1, steps))
+        # the force records are sums of FP64 atomics from many blocks: their order, and so the
+        # last bits, vary from run to run
+        fa, fb = a.force_history(1, steps), b.force_history(1, steps)
+        assert np.linalg.norm(fa - fb) <= 1e-12 * np.linalg.norm(fb) + 1e-15
     finally:
         a.close()
         b.close()
@@ -212,7 +217,10 @@ def test_octo_even_kernel_matches_quad_kernel(gpu, steps):
     a, b = run(True), run(False)
     try:
         assert np.array_equal(a.populations(np.float32), b.populations(np.float32))
-        assert np.array_equal(a.force_history(1, steps), b.force_history(1, steps))
+        # the force records are sums of FP64 atomics from many blocks: their order, and so the
+        # last bits, vary from run to run
+        fa, fb = a.force_history(1, steps), b.force_history(1, steps)
+        assert np.linalg.norm(fa - fb) <= 1e-12 * np.linalg.norm(fb) + 1e-15
     finally:
         a.close()
         b.close()
