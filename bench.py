@@ -79,7 +79,9 @@ def step_kernel(storage: str, n: int) -> str:
         return "aa_step_kernel"
     if storage == "fp16dev":
         quad = os.environ.get("LBM3D_QUAD") != "0"
-        return ("aa_quad_even_kernel" if quad else "aa_pair_kernel") + " / aa_pair_split_kernel"
+        octo = quad and n % 256 == 0 and os.environ.get("LBM3D_OCTO") != "0"
+        even = "aa_octo_even_kernel" if octo else ("aa_quad_even_kernel" if quad else "aa_pair_kernel")
+        return even + " / aa_pair_split_kernel"
     return "aa_pair_kernel"
 
 

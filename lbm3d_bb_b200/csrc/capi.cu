@@ -760,9 +760,9 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     const char* q = std::getenv("LBM3D_QUAD");
     c->quad = c->pair && cfg->storage == LBM_STORE_FP16DEV && !(q && q[0] == '0');
     // eight cells per thread in the FP16-deviation even phase (16-byte words; nx a multiple
-    // of 256): LBM3D_OCTO=1
+    // of 256; 6 % faster than four cells on the 512^3 box on B200); LBM3D_OCTO=0 keeps four
     const char* oc = std::getenv("LBM3D_OCTO");
-    c->octo = c->quad && cfg->nx % 256 == 0 && (oc && oc[0] == '1');
+    c->octo = c->quad && cfg->nx % 256 == 0 && !(oc && oc[0] == '0');
     // FP32 odd phase with the x-shifted directions moved as shuffled two-element words:
     // LBM3D_XSHUFFLE=1 (5 % slower than the pair kernel on the 512^3 box on B200)
     const char* xs = std::getenv("LBM3D_XSHUFFLE");

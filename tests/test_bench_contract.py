@@ -32,7 +32,7 @@ def test_reference_arm_line():
 
 def test_roofline_traffic_comes_from_the_committed_summaries():
     assert bench.step_kernel("fp32", 512) == "aa_pair_kernel"
-    assert bench.step_kernel("fp16dev", 512) == "aa_quad_even_kernel / aa_pair_split_kernel"
+    assert bench.step_kernel("fp16dev", 512) == "aa_octo_even_kernel / aa_pair_split_kernel"
     assert bench.step_kernel("fp64", 512) == "aa_step_kernel"
     for storage, algorithmic in (("fp32", 153), ("fp16dev", 77)):
         t = bench.profiled_traffic(storage, 512)

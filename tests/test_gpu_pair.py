@@ -187,10 +187,11 @@ def test_fp32_shuffled_odd_phase_matches_pair_kernel(gpu, nx, steps, collision):
     a, b = run(True), run(False)
     try:
         assert np.array_equal(a.populations(np.float32), b.populations(np.float32))
-        # the force records are sums of FP64 atomics from many blocks: their order, and so the
-        # last bits, vary from run to run
+        # the force records are FP64 sums over links, grouped per thread and block and added
+        # by atomics: a different grouping (or atomic order) moves the last bits; the force
+        # bound of the parity contract applies
         fa, fb = a.force_history(1, steps), b.force_history(1, steps)
-        assert np.linalg.norm(fa - fb) <= 1e-12 * np.linalg.norm(fb) + 1e-15
+        assert np.linalg.norm(fa - fb) <= 1e-9 * np.linalg.norm(fb) + 1e-15
     finally:
         a.close()
         b.close()
@@ -198,9 +199,10 @@ def test_fp32_shuffled_odd_phase_matches_pair_kernel(gpu, nx, steps, collision):
 
 @pytest.mark.parametrize("steps", [4, 7])
 def test_octo_even_kernel_matches_quad_kernel(gpu, steps):
-    """FP16-deviation even phase with eight cells per thread and 16-byte words
-    (LBM3D_OCTO=1, nx a multiple of 256) against the four-cell kernel: the same per-cell
-    arithmetic, so the same bits; the porous box mixes plain and boundary warps."""
+    """FP16-deviation even phase with eight cells per thread and 16-byte words (default for
+    nx a multiple of 256; LBM3D_OCTO=0 keeps the four-cell kernel) against the four-cell
+    kernel: the same per-cell arithmetic, so the same bits; the porous box mixes plain and
+    boundary warps."""
     var = "LBM3D_OCTO"
 
     def run(on):
@@ -217,10 +219,11 @@ def test_octo_even_kernel_matches_quad_kernel(gpu, steps):
     a, b = run(True), run(False)
     try:
         assert np.array_equal(a.populations(np.float32), b.populations(np.float32))
-        # the force records are sums of FP64 atomics from many blocks: their order, and so the
-        # last bits, vary from run to run
+        # the force records are FP64 sums over links, grouped per thread and block and added
+        # by atomics: a different grouping (or atomic order) moves the last bits; the force
+        # bound of the parity contract applies
         fa, fb = a.force_history(1, steps), b.force_history(1, steps)
-        assert np.linalg.norm(fa - fb) <= 1e-12 * np.linalg.norm(fb) + 1e-15
+        assert np.linalg.norm(fa - fb) <= 1e-9 * np.linalg.norm(fb) + 1e-15
     finally:
         a.close()
         b.close()
