@@ -1442,18 +1442,52 @@ __global__ void __launch_bounds__(128, 3) aa_octo_even_kernel(const __grid_const
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
 
+// Ordinal (0..9) of an x-shifted D3Q19 direction among the ten.
+__host__ __device__ constexpr int xslot(int d) {
+  int n = 0;
+  for (int e = 0; e < d; e++) n += cx(e) != 0 ? 1 : 0;
+  return n;
+}
+
+// The split pair update of `pairs` cell pairs from x0 (blocks off the word path); out of
+// line, which keeps the word path's code compact.
+template <bool TRT, int FORCE>
+__device__ __noinline__ void odd_pairs_fallback(const AAParams& p, __half* __restrict__ A,
+                                                const uint8_t* __restrict__ flags, const int x0, const int pairs,
+                                                const int y, const int z, const bool inb, double* acc, bool* has_out) {
+  bool has_link = *has_out;
+#pragma unroll 1
+  for (int h = 0; h < pairs; h++) pair_split_cells<StF16, TRT, FORCE>(p, A, flags, x0 + 2 * h, y, z, inb, acc, has_link);
+  *has_out = has_link;
+}
+
+// Stores the elements of an 8-byte word whose bit in `skip` is clear (2-byte elements; q
+// 8-byte aligned).
+__device__ __forceinline__ void st_u2_masked(char* q, const uint2 v, const uint32_t skip) {
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+    if (!((skip >> k) & 1u))
+      *reinterpret_cast<unsigned short*>(q + 2 * k) = (unsigned short)((k < 2 ? v.x : v.y) >> (16 * (k & 1)));
+}
+
 // ---- quad kernel: odd phase, FP16-deviation storage ----------------------------------
-// One thread updates four x-adjacent cells (x0 .. x0+3, x0 a multiple of 4) and a warp 128
-// consecutive cells of one row.  Every direction moves as one aligned 8-byte word per
-// thread and direction (19 loads and 19 stores for four cells): for an x-shifted direction
-// the word of the same four positions is shifted by one element, the element that enters
-// from the neighbouring thread's word comes by warp shuffle, and only the warp's edge lanes
-// move one more element through memory (lane 0 and lane 31, with the periodic x wrap).
-// Every slot is still read and written by exactly one thread: an aligned word that a warp
-// covers only in part (its first element for pushes along +x, its last for pushes along -x)
-// gets the missing element from the neighbouring warp's edge lane.  Warps holding a solid,
-// near-boundary or uncovered cell, or a row next to a y/z wrap, run the split pair update on
-// their two cell pairs instead.
+// One block holds whole rows: nx / 4 threads per row (nx a multiple of 128, at most 1024),
+// four x-adjacent cells per thread (x0 a multiple of 4), at most 256 threads.  Every
+// direction moves as one aligned 8-byte word per thread: for an x-shifted direction the word
+// of the thread's own four positions is shifted by one element, and the element that enters
+// comes from the neighbouring thread of the row through shared memory (the last thread of a
+// row neighbours the first: periodic x); every thread takes part, so the exchange has no
+// divergent branch.  The outputs are shifted back the same way before the 19 word stores.
+// Solid cells are collided with whatever their slots hold and left out when the words are
+// stored: a word that carries a solid cell's output is stored element by element without
+// it, because that element would land on the own slot where the fluid neighbour keeps its
+// bounce-back value.  Fluid cells next to a solid (static links) stay on the word path:
+// they take their bounce-back inputs from their own slots and write the outputs that point
+// into a solid to their own slots; the word elements they push into a solid node's slot
+// are dead (no cell reads them while the node is solid).  Every other slot is read and
+// written by exactly the thread of the cell whose pull/push set holds it.  Blocks holding a
+// cell with a moving or changed link, an uncovered cell, or a row next to a y/z wrap (or
+// past ny) run the split pair update instead (block vote).
 template <bool TRT, int FORCE>
 __global__ void __launch_bounds__(256, 2) aa_quad_odd_kernel(const __grid_constant__ AAParams p,
                                                              __half* __restrict__ A,
@@ -1461,57 +1495,78 @@ __global__ void __launch_bounds__(256, 2) aa_quad_odd_kernel(const __grid_consta
   using SP = StF16;
   using C = float;
   const Grid& g = p.g;
-  const int lane = threadIdx.x;  // blockDim.x == 32: one warp is one row segment
-  const int x0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  // this thread and its x neighbours in the row (periodic) in the exchange arrays
+  const int nxt = (int)blockDim.x;  // threads per row
+  const int tid = (int)threadIdx.x + nxt * (int)threadIdx.y;
+  const int tprev = tid + ((int)threadIdx.x == 0 ? nxt - 1 : -1);
+  const int tnext = tid + ((int)threadIdx.x == nxt - 1 ? 1 - nxt : 1);
+  const int x0 = 4 * (int)threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
-  const bool inb = x0 < g.nx && y < g.ny;
+  const bool inb = y < g.ny;
   clear_record(p.zero_next);
   if (ghost_plane(p, z)) return;  // whole block in a ghost plane
+  // exchange: the element of each x-shifted direction (slot xslot(d)) that enters the
+  // neighbouring thread's word, and the solid masks
+  __shared__ unsigned short xin[10][256], xout[10][256];
+  __shared__ unsigned char xsk[256];
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   bool has_link = false;
   const long long i0 = inb ? node_index(g, x0, y, z) : 0;
   uint32_t fw = 0x01010101u * F_SOLID;
   if (inb) fw = *reinterpret_cast<const uint32_t*>(flags + i0);
-  // four fluid cells away from any solid (F_SOLID, F_SOLID_PREV, F_NEAR clear), not in a
-  // row next to the y/z wrap
-  const bool plain = inb && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1 && (fw & 0x07070707u) == 0u;
-  if (__all_sync(0xffffffffu, plain)) {
+  uint32_t smask = 0;  // bit k: cell x0 + k is solid
+  bool fast = inb && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t fl = (fw >> (8 * k)) & 0xFFu;
+    if (fl & F_SOLID) {
+      smask |= 1u << k;
+    } else {
+      if (fl & F_SOLID_PREV) fast = false;
+      if (fl & F_NEAR) {
+        const unsigned long long lw = p.links[i0 + k];
+        fast = fast && (uint32_t)(lw & 0x3FFFFu) == (uint32_t)((lw >> 18) & 0x3FFFFu) && ((lw >> 36) & 0x3FFFFu) == 0;
+      }
+    }
+  }
+  if (__syncthreads_and(fast)) {
     char* const Ai = reinterpret_cast<char*>(A + i0);
-    const long long wrap_lo = x0 == 0 ? 2LL * g.nx : 0;           // element x0 - 1 at x = nx - 1
-    const long long wrap_hi = x0 + 4 == g.nx ? 2LL * g.nx : 0;    // element x0 + 4 at x = 0
+    const C rho0 = C(p.rho0);
     uint2 w[Q];
-    unsigned short edge[Q];
 #pragma unroll
     for (int d = 0; d < Q; d++) {
-      const long long o = p.offb_rd[d];
-      if (cx(d) == 0) {
-        w[d] = *reinterpret_cast<const uint2*>(Ai + o);
-      } else if (cx(d) == 1) {  // pull from x - 1: o addresses element x0 - 1 of the source row
-        w[d] = *reinterpret_cast<const uint2*>(Ai + o + 2);
-        if (lane == 0) edge[d] = *reinterpret_cast<const unsigned short*>(Ai + o + wrap_lo);
-      } else {  // pull from x + 1: o addresses element x0 + 1
-        w[d] = *reinterpret_cast<const uint2*>(Ai + o - 2);
-        if (lane == 31) edge[d] = *reinterpret_cast<const unsigned short*>(Ai + o + 6 - wrap_hi);
-      }
+      // offb_rd addresses element x0 - c_dx of the source row: the aligned word is at x0
+      w[d] = *reinterpret_cast<const uint2*>(Ai + p.offb_rd[d] + 2 * cx(d));
     }
-    // shift the x-pulled words by one element (element k = bits 16k .. 16k+15)
 #pragma unroll
     for (int d = 0; d < Q; d++) {
-      if (cx(d) == 1) {  // [x0-1, x0, x0+1, x0+2]: the last element of the previous lane's word
-        const uint32_t up = __shfl_up_sync(0xffffffffu, w[d].y, 1) >> 16;
-        const uint32_t in = lane == 0 ? (uint32_t)edge[d] : up;
-        w[d] = make_uint2((w[d].x << 16) | in, __funnelshift_l(w[d].x, w[d].y, 16));
-      } else if (cx(d) == -1) {  // [x0+1 .. x0+4]: the first element of the next lane's word
-        const uint32_t dn = __shfl_down_sync(0xffffffffu, w[d].x, 1) & 0xFFFFu;
-        const uint32_t in = lane == 31 ? (uint32_t)edge[d] : dn;
-        w[d] = make_uint2(__funnelshift_r(w[d].x, w[d].y, 16), (w[d].y >> 16) | (in << 16));
+      if (cx(d) == 1) xin[xslot(d)][tid] = (unsigned short)(w[d].y >> 16);      // last element
+      if (cx(d) == -1) xin[xslot(d)][tid] = (unsigned short)(w[d].x & 0xFFFFu);  // first element
+    }
+    xsk[tid] = (unsigned char)smask;
+    __syncthreads();
+    // shift the x-pulled words by one element (element k = bits 16(k%2) of 32-bit word k/2)
+#pragma unroll
+    for (int d = 0; d < Q; d++) {
+      const uint2 v = w[d];
+      if (cx(d) == 1) {  // [x0-1 .. x0+2]: the last element of the previous thread's word
+        const uint32_t in = xin[xslot(d)][tprev];
+        w[d] = make_uint2((v.x << 16) | in, __funnelshift_l(v.x, v.y, 16));
+      } else if (cx(d) == -1) {  // [x0+1 .. x0+4]: the first element of the next thread's word
+        const uint32_t in = xin[xslot(d)][tnext];
+        w[d] = make_uint2(__funnelshift_r(v.x, v.y, 16), (v.y >> 16) | (in << 16));
       }
     }
-    // collide the cells in pairs (low and high half2 of each 32-bit word)
-    uint2 out[Q];
+    // collide the cells in pairs (low and high half2 of each 32-bit word); each pair's
+    // outputs replace its inputs in the words.  Solid cells compute values that are never
+    // stored.
 #pragma unroll
     for (int h = 0; h < 2; h++) {
+      const int ka = 2 * h, kb = 2 * h + 1;
+      const uint32_t fla = (fw >> (16 * h)) & 0xFFu, flb = (fw >> (16 * h + 8)) & 0xFFu;
+      const uint32_t bca = (fla & F_NEAR) && !(fla & F_SOLID) ? (uint32_t)(p.links[i0 + ka] & 0x3FFFFu) : 0u;
+      const uint32_t bcb = (flb & F_NEAR) && !(flb & F_SOLID) ? (uint32_t)(p.links[i0 + kb] & 0x3FFFFu) : 0u;
       C pa[Q], pb[Q];
       {
         C f[Q];
@@ -1519,6 +1574,11 @@ __global__ void __launch_bounds__(256, 2) aa_quad_odd_kernel(const __grid_consta
         for (int d = 0; d < Q; d++) {
           const uint32_t u = h ? w[d].y : w[d].x;
           f[d] = __low2float(*reinterpret_cast<const __half2*>(&u));
+        }
+        if (bca) {  // bounce-back values are kept in the own slots
+#pragma unroll
+          for (int d = 0; d < 18; d++)
+            if ((bca >> d) & 1u) f[d] = ld_fast<SP>(A + (long long)d * g.plane + i0 + ka, d, rho0);
         }
         pair_cell<SP, true, TRT, FORCE>(p, f, pa);
       }
@@ -1529,6 +1589,11 @@ __global__ void __launch_bounds__(256, 2) aa_quad_odd_kernel(const __grid_consta
           const uint32_t u = h ? w[d].y : w[d].x;
           f[d] = __high2float(*reinterpret_cast<const __half2*>(&u));
         }
+        if (bcb) {
+#pragma unroll
+          for (int d = 0; d < 18; d++)
+            if ((bcb >> d) & 1u) f[d] = ld_fast<SP>(A + (long long)d * g.plane + i0 + kb, d, rho0);
+        }
         pair_cell<SP, true, TRT, FORCE>(p, f, pb);
       }
 #pragma unroll
@@ -1536,43 +1601,56 @@ __global__ void __launch_bounds__(256, 2) aa_quad_odd_kernel(const __grid_consta
         const __half2 v = __floats2half2_rn(pa[j], pb[j]);
         const uint32_t u = *reinterpret_cast<const uint32_t*>(&v);
         if (h)
-          out[j].y = u;
+          w[j].y = u;
         else
-          out[j].x = u;
+          w[j].x = u;
+      }
+      if (bca | bcb) {  // outputs into a solid go to the own slots
+#pragma unroll
+        for (int j = 0; j < 18; j++) {
+          const int oj = opp(j);
+          if ((bca >> oj) & 1u) st_fast<SP>(A + (long long)oj * g.plane + i0 + ka, pa[j], j, rho0);
+          if ((bcb >> oj) & 1u) st_fast<SP>(A + (long long)oj * g.plane + i0 + kb, pb[j], j, rho0);
+        }
+        if (p.compute_force) {
+          pair_links<SP>(p, x0 + ka, y, z, bca, pa, acc);
+          pair_links<SP>(p, x0 + kb, y, z, bcb, pb, acc);
+          has_link = true;
+        }
       }
     }
 #pragma unroll
     for (int j = 0; j < Q; j++) {
-      const long long o = p.offb_wr[j];
-      if (cx(j) == 0) {
-        *reinterpret_cast<uint2*>(Ai + o) = out[j];
-      } else if (cx(j) == 1) {  // push to x + 1: o addresses element x0 + 1 of the target row
-        const uint32_t up = __shfl_up_sync(0xffffffffu, out[j].y, 1) >> 16;
-        if (lane != 0) {
-          *reinterpret_cast<uint2*>(Ai + o - 2) =
-              make_uint2((out[j].x << 16) | up, __funnelshift_l(out[j].x, out[j].y, 16));
-        } else {  // elements x0+1 .. x0+3; element x0 comes from the previous warp's lane 31
-          *reinterpret_cast<unsigned short*>(Ai + o) = (unsigned short)(out[j].x & 0xFFFFu);
-          *reinterpret_cast<uint32_t*>(Ai + o + 2) = __funnelshift_l(out[j].x, out[j].y, 16);
-        }
-        if (lane == 31)  // the fourth cell's value lands in the next warp's first word
-          *reinterpret_cast<unsigned short*>(Ai + o + 6 - wrap_hi) = (unsigned short)(out[j].y >> 16);
-      } else {  // push to x - 1: o addresses element x0 - 1
-        const uint32_t dn = __shfl_down_sync(0xffffffffu, out[j].x, 1) & 0xFFFFu;
-        if (lane != 31) {
-          *reinterpret_cast<uint2*>(Ai + o + 2) =
-              make_uint2(__funnelshift_r(out[j].x, out[j].y, 16), (out[j].y >> 16) | (dn << 16));
-        } else {  // elements x0 .. x0+2; element x0+3 comes from the next warp's lane 0
-          *reinterpret_cast<uint32_t*>(Ai + o + 2) = __funnelshift_r(out[j].x, out[j].y, 16);
-          *reinterpret_cast<unsigned short*>(Ai + o + 6) = (unsigned short)(out[j].y >> 16);
-        }
-        if (lane == 0)  // the first cell's value lands in the previous warp's last word
-          *reinterpret_cast<unsigned short*>(Ai + o + wrap_lo) = (unsigned short)(out[j].x & 0xFFFFu);
+      if (cx(j) == 1) xout[xslot(j)][tid] = (unsigned short)(w[j].y >> 16);      // the fourth cell's output
+      if (cx(j) == -1) xout[xslot(j)][tid] = (unsigned short)(w[j].x & 0xFFFFu);  // the first cell's output
+    }
+    __syncthreads();
+    // solid cells among the six whose outputs the stored words carry: bit 0 = cell x0 - 1,
+    // bits 1..4 = cells x0 .. x0+3, bit 5 = cell x0 + 4
+    const uint32_t win = (((uint32_t)xsk[tprev] >> 3) & 1u) | (smask << 1) | (((uint32_t)xsk[tnext] & 1u) << 5);
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+      const uint2 v = w[j];
+      uint2 nw = v;
+      uint32_t skip = (win >> 1) & 0xFu;  // cells x0 .. x0+3
+      if (cx(j) == 1) {  // push to x + 1: the word at x0 carries cells x0-1 .. x0+2
+        const uint32_t in = xout[xslot(j)][tprev];
+        nw = make_uint2((v.x << 16) | in, __funnelshift_l(v.x, v.y, 16));
+        skip = win & 0xFu;
+      } else if (cx(j) == -1) {  // push to x - 1: the word at x0 carries cells x0+1 .. x0+4
+        const uint32_t in = xout[xslot(j)][tnext];
+        nw = make_uint2(__funnelshift_r(v.x, v.y, 16), (v.y >> 16) | (in << 16));
+        skip = (win >> 2) & 0xFu;
       }
+      // offb_wr addresses element x0 + c_jx of the target row: the aligned word is at x0
+      char* const q = Ai + p.offb_wr[j] - 2 * cx(j);
+      if (skip == 0u)
+        *reinterpret_cast<uint2*>(q) = nw;
+      else
+        st_u2_masked(q, nw, skip);
     }
   } else {
-    pair_split_cells<SP, TRT, FORCE>(p, A, flags, x0, y, z, inb, acc, has_link);
-    pair_split_cells<SP, TRT, FORCE>(p, A, flags, x0 + 2, y, z, inb, acc, has_link);
+    odd_pairs_fallback<TRT, FORCE>(p, A, flags, x0, 2, y, z, inb, acc, &has_link);
   }
   if (p.compute_force) block_force_reduce(acc, has_link, p.force + block_stripe());
 }
@@ -1980,8 +2058,10 @@ static cudaError_t launch_one(const AAParams& p, void* A, const uint8_t* flags, 
     if (p.pair) {  // 64 x 4 threads, two cells each
       const dim3 pb(64, 4, 1), pg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 3) / 4), (unsigned)p.g.nz);
       if constexpr (ODD && SP::DEV) {
-        if (p.quad) {  // 32 x 8 threads, four cells each
-          const dim3 qb(32, 8, 1), qg((unsigned)(p.g.nx / 128), (unsigned)((p.g.ny + 7) / 8), (unsigned)p.g.nz);
+        if (p.quad) {  // whole rows: nx / 4 threads each, 128 threads (nx at most 512) or one row
+          const int rows = p.g.nx <= 512 ? 512 / p.g.nx : 1;
+          const dim3 qb((unsigned)(p.g.nx / 4), (unsigned)rows, 1),
+              qg(1u, (unsigned)((p.g.ny + rows - 1) / rows), (unsigned)p.g.nz);
           aa_quad_odd_kernel<TRT, FORCE><<<qg, qb, 0, s>>>(p, (__half*)A, flags);
         } else {
           aa_pair_split_kernel<SP, TRT, FORCE><<<pg, pb, 0, s>>>(p, (typename SP::S*)A, flags);

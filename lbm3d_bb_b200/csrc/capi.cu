@@ -767,10 +767,11 @@ int32_t lbm_create(const lbm_config* cfg, int32_t device, lbm_ctx** out) {
     // LBM3D_XSHUFFLE=1 (5 % slower than the pair kernel on the 512^3 box on B200)
     const char* xs = std::getenv("LBM3D_XSHUFFLE");
     c->xshuffle = c->pair && cfg->storage == LBM_STORE_FP32 && (xs && xs[0] == '1');
-    // FP16-deviation odd phase on four cells per thread: LBM3D_QUAD_ODD=1 (9 % slower than
-    // the split pair kernel on the 512^3 box on B200)
+    // FP16-deviation odd phase on four cells per thread (8-byte words, x shifts exchanged
+    // through shared memory; blocks of whole rows, nx at most 1024): LBM3D_QUAD_ODD=1 (22 %
+    // slower than the split pair kernel on the 512^3 box on B200)
     const char* qo = std::getenv("LBM3D_QUAD_ODD");
-    c->quad_odd = c->quad && (qo && qo[0] == '1');
+    c->quad_odd = c->quad && cfg->nx <= 1024 && (qo && qo[0] == '1');
   }
   c->bytes += fl + ring_bytes + 64;
   if (c->cuda(cudaMemset(c->flags, 0, fl), "memset flags")) return bail(LBM_ERR_CUDA);

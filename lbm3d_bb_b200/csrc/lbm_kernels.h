@@ -41,7 +41,7 @@ struct AAParams {
   // on the fast path, everything else takes the general path
   const unsigned long long* links;
   int pair;  // all axes periodic, nx % 128 == 0: two cells per thread (aa_pair_kernel)
-  int quad;  // with pair, FP16-deviation: four cells per thread (aa_quad_even_kernel, aa_quad_odd_kernel)
+  int quad;  // with pair, FP16-deviation: 1 four cells per thread (aa_quad_even/odd_kernel), 2 eight in the even phase (aa_octo_even_kernel)
   int xshuffle;  // with pair, FP32 odd phase: x-shifted directions as shuffled words (aa_pair_odd_kernel)
 };
 

@@ -90,9 +90,9 @@ def test_pair_kernel_vs_oracle(gpu, oracle_lib, storage):
 @pytest.mark.parametrize("collision", ["BGK", "TRT"])
 def test_quad_kernels_match_pair_kernels(gpu, steps, nx, collision):
     """FP16-deviation with four cells per thread in both phases (LBM3D_QUAD, default on:
-    aa_quad_even_kernel; with LBM3D_QUAD_ODD=1 also aa_quad_odd_kernel with its word shifts,
-    warp shuffles and edge-lane elements, one or two warps per row) against the pair
-    kernels: same populations to storage rounding, same force history."""
+    aa_quad_even_kernel; with LBM3D_QUAD_ODD=1 also aa_quad_odd_kernel with its word shifts
+    exchanged through shared memory, one block per set of rows) against the pair kernels:
+    same populations to storage rounding, same force history."""
     kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
     var = "LBM3D_QUAD"
 
@@ -224,6 +224,80 @@ def test_octo_even_kernel_matches_quad_kernel(gpu, steps):
         # bound of the parity contract applies
         fa, fb = a.force_history(1, steps), b.force_history(1, steps)
         assert np.linalg.norm(fa - fb) <= 1e-9 * np.linalg.norm(fb) + 1e-15
+    finally:
+        a.close()
+        b.close()
+
+
+def _with_env(var, value, fn):
+    old = os.environ.get(var)
+    os.environ[var] = value
+    try:
+        return fn()
+    finally:
+        if old is None:
+            del os.environ[var]
+        else:
+            os.environ[var] = old
+
+
+@pytest.mark.parametrize("var,nx", [("LBM3D_QUAD_ODD", 512), ("LBM3D_QUAD_ODD", 128), ("LBM3D_QUAD_ODD", 384),
+                                    ("LBM3D_QUAD_ODD", 1024)])
+@pytest.mark.parametrize("steps", [2, 7])
+@pytest.mark.parametrize("collision", ["BGK", "TRT"])
+def test_word_odd_kernel_matches_split_kernel(gpu, var, nx, steps, collision):
+    """FP16-deviation odd phase on aligned words with the x shifts exchanged between the
+    threads of a row (LBM3D_QUAD_ODD=1: aa_quad_odd_kernel, four cells per thread) against
+    the split pair kernel: solid cells and static links on the word path, rows next to the
+    y/z wrap on the split pair update; the same per-cell arithmetic, so the same bits.  One
+    to eight warps per row and one to four rows per block cover the exchange and the
+    periodic x wrap."""
+    kw = {} if collision == "BGK" else {"omega_m": 1.0 / (0.5 + 0.1875 / (0.6 - 0.5))}
+
+    def run(on):
+        return _with_env(var, "1" if on else "0",
+                         lambda: _porous(Domain, steps, "fp16dev", nx=nx, ny=12, nz=10, seed=23, **kw))
+
+    a, b = run(True), run(False)
+    try:
+        assert np.array_equal(a.populations(np.float32), b.populations(np.float32))
+        # the force records are FP64 sums over links, grouped per thread and block and added
+        # by atomics: a different grouping (or atomic order) moves the last bits
+        fa, fb = a.force_history(1, steps), b.force_history(1, steps)
+        assert np.linalg.norm(fa - fb) <= 1e-9 * np.linalg.norm(fb) + 1e-15
+        a.check_finite()
+    finally:
+        a.close()
+        b.close()
+
+
+def test_word_odd_kernel_moving_body_matches_split_kernel(gpu):
+    """The same comparison with a sphere moving through the periodic box: blocks with
+    uncovered cells or changed links take the split pair update inside the word kernel.
+    The vote that sends cells to the general path covers a block of rows in the word
+    kernel and a warp in the split kernel, so a few more cells near the body run the general path,
+    which computes FP16-deviation storage in absolute form: rounding level."""
+    from lbm3d_bb_b200 import abi
+
+    def run(on):
+        def go():
+            d = Domain(256, 24, 20, collision="BGK", storage="fp16dev", faces=cases.PERIODIC, omega_p=1.0 / 0.6,
+                       accel=(1e-5, 0.0, 0.0), compute_force=True)
+            d.add_body(abi.make_body(abi.BODY_SPHERE, (60.0, 12.0, 10.0), radius=5.0, moving=True))
+            d.init_equilibrium()
+            for n in range(1, 13):
+                at = lambda t: abi.make_pose(center=(60.0 + 0.3 * t, 12.0, 10.0), vel=(0.3, 0.0, 0.0))
+                d.update_body(at(n - 1.0), at(n - 0.5))
+                d.step(1)
+            return d
+        return _with_env("LBM3D_QUAD_ODD", "1" if on else "0", go)
+
+    a, b = run(True), run(False)
+    try:
+        assert rel_l2(a.populations(), b.populations()) <= TOL["fp16dev"]
+        fa, fb = a.force_history(1, 12)[:, :3], b.force_history(1, 12)[:, :3]
+        assert np.linalg.norm(fa - fb) <= 10 * TOL["fp16dev"] * np.linalg.norm(fb) + 1e-11
+        a.check_finite()
     finally:
         a.close()
         b.close()
