@@ -575,6 +575,38 @@ __device__ __forceinline__ void aa_fast_load(const AAParams& p, const typename S
   }
 }
 
+// Momentum exchange of one cell's static bounce-back links (bit d of bc: incoming d, source
+// solid): each link o = opp(d) carries c_o (f*_o + f*_o).  The links' torque is r_cell x
+// F_cell with r_cell the cell centre relative to the torque centre: the half-link offsets
+// 0.5 c_o drop out because c_o x c_o = 0, so a link costs one addition per nonzero component.
+template <class SP>
+__device__ __forceinline__ void pair_links(const AAParams& p, const int x, const int y, const int z, const uint32_t bc,
+                                           const typename SP::C* pst, double* acc) {
+  using C = typename SP::C;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+#pragma unroll
+  for (int d = 0; d < 18; d++) {
+    if (!((bc >> d) & 1u)) continue;
+    const int o = opp(d);
+    const double t = 2.0 * (double)(SP::DEV ? pst[o] + wgt<C>(o) * C(p.rho0) : pst[o]);
+    if (cx(o) > 0) fx += t;
+    if (cx(o) < 0) fx -= t;
+    if (cy(o) > 0) fy += t;
+    if (cy(o) < 0) fy -= t;
+    if (cz(o) > 0) fz += t;
+    if (cz(o) < 0) fz -= t;
+  }
+  const double rx = x + 0.5 - p.kin.center[0];
+  const double ry = y + 0.5 - p.kin.center[1];
+  const double rz = z + 0.5 - p.kin.center[2];
+  acc[0] += fx;
+  acc[1] += fy;
+  acc[2] += fz;
+  acc[3] += ry * fz - rz * fy;
+  acc[4] += rz * fx - rx * fz;
+  acc[5] += rx * fy - ry * fx;
+}
+
 template <class SP, bool ODD, bool TRT, int FORCE, bool FACES>
 __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S* __restrict__ base,
                                                const int x, const int y, const int z, const uint32_t bc,
@@ -640,23 +672,7 @@ __device__ __forceinline__ void aa_fast_finish(const AAParams& p, typename SP::S
     }
   }
   if (bc && p.compute_force) {
-    // momentum exchange of the static links: c_o (f*_o + f*_o), o = opp(d)
-#pragma unroll
-    for (int d = 0; d < 18; d++) {
-      if (!((bc >> d) & 1u)) continue;
-      const int o = opp(d);
-      const double t = 2.0 * (double)(SP::DEV ? pst[o] + wgt<C>(o) * rho0 : pst[o]);
-      const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
-      const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
-      const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
-      const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
-      acc[0] += fx;
-      acc[1] += fy;
-      acc[2] += fz;
-      acc[3] += ry * fz - rz * fy;
-      acc[4] += rz * fx - rx * fz;
-      acc[5] += rx * fy - ry * fx;
-    }
+    pair_links<SP>(p, x, y, z, bc, pst, acc);  // momentum exchange of the static links
     *has_link = true;
   }
 }
@@ -794,28 +810,6 @@ __device__ __forceinline__ void pair_cell(const AAParams& p, const typename SP::
   C rho, ux, uy, uz;
   moments<C, FORCE, SP::DEV>(f, k, rho, ux, uy, uz, rho0);
   collide<C, TRT, FORCE, SP::DEV>(f, pst, k, rho, ux, uy, uz, rho0);
-}
-
-template <class SP>
-__device__ __forceinline__ void pair_links(const AAParams& p, const int x, const int y, const int z, const uint32_t bc,
-                                           const typename SP::C* pst, double* acc) {
-  using C = typename SP::C;
-#pragma unroll
-  for (int d = 0; d < 18; d++) {
-    if (!((bc >> d) & 1u)) continue;
-    const int o = opp(d);
-    const double t = 2.0 * (double)(SP::DEV ? pst[o] + wgt<C>(o) * C(p.rho0) : pst[o]);
-    const double fx = t * cx(o), fy = t * cy(o), fz = t * cz(o);
-    const double rx = x + 0.5 + 0.5 * cx(o) - p.kin.center[0];
-    const double ry = y + 0.5 + 0.5 * cy(o) - p.kin.center[1];
-    const double rz = z + 0.5 + 0.5 * cz(o) - p.kin.center[2];
-    acc[0] += fx;
-    acc[1] += fy;
-    acc[2] += fz;
-    acc[3] += ry * fz - rz * fy;
-    acc[4] += rz * fx - rx * fz;
-    acc[5] += rx * fy - ry * fx;
-  }
 }
 
 // The update of the cell pair (x0, x0 + 1), x0 even, as described above; all 32 lanes of the
