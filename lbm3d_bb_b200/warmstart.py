@@ -256,7 +256,8 @@ def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int 
             newly = (~done) & (ch < tol)
             steps[newly] = st.steps
             done |= newly | ~np.isfinite(ch)
-        st.batch.synchronize()
+            st.retire(done)  # settled or diverged cases stop stepping
+        torch.cuda.synchronize()
         log(f"group {g0 // group}: {len(params)} cases, {st.steps} steps, {time.perf_counter() - t0:.1f} s, "
             f"converged {(steps > 0).sum()}")
         for k, (p, d) in enumerate(zip(params, st.doms)):
