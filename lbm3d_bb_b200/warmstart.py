@@ -398,6 +398,9 @@ def main(argv=None):
     ap.add_argument("--rho-weight", type=float, default=1.0, help="loss weight of the density channel")
     ap.add_argument("--augment", action="store_true", help="train on the three mirror images of every state too")
     ap.add_argument("--mirror-average", action="store_true", help="average the prediction over the four mirror images")
+    ap.add_argument("--time-budget", type=float, default=0.0,
+                    help="wall seconds for the whole run: fewer epochs when training would not fit (0: no limit)")
+    ap.add_argument("--eval-reserve", type=float, default=900.0, help="seconds kept for the evaluation under --time-budget")
     ap.add_argument("--out", default="warmstart_out")
     ap.add_argument("--eval-weights", default=None,
                     help="evaluate these saved weights on the held-out seeds (no data generation or training)")
@@ -434,9 +437,28 @@ def _run(args, stream, out, log):
         X, T, M, counts, rec = generate(train_seeds, 0, stream, args.max_steps, args.tol, log=log,
                                         augment=args.augment)
         log(f"training set: {X.shape[0]} steady states of {len(train_seeds)} ({time.perf_counter() - t0:.0f} s)")
+        epochs = args.epochs
+        if args.time_budget > 0:
+            # time a few training steps on a scratch network, then fit the epochs (and with
+            # them the cosine schedule) into what is left of the budget
+            probe = UNet3D(16, 0, stream, seed=1)
+            train(probe, X[:8 * args.batch], T[:8 * args.batch], M[:8 * args.batch], counts[:8 * args.batch], 1,
+                  args.batch, args.lr, log=lambda m: None)
+            torch.cuda.synchronize()
+            tp = time.perf_counter()
+            train(probe, X[:8 * args.batch], T[:8 * args.batch], M[:8 * args.batch], counts[:8 * args.batch], 1,
+                  args.batch, args.lr, log=lambda m: None)
+            torch.cuda.synchronize()
+            step_s = (time.perf_counter() - tp) / 8
+            del probe
+            left = args.time_budget - (time.perf_counter() - t0) - args.eval_reserve
+            fit = int(left / (step_s * max(1, X.shape[0] // args.batch)))
+            epochs = max(1, min(args.epochs, fit))
+            log(f"time budget: {step_s * 1e3:.1f} ms per training step, {left:.0f} s left for training: "
+                f"{epochs} epochs")
         model = UNet3D(16, 0, stream, seed=0)
         t1 = time.perf_counter()
-        hist = train(model, X, T, M, counts, args.epochs, args.batch, args.lr, log=log,
+        hist = train(model, X, T, M, counts, epochs, args.batch, args.lr, log=log,
                      weights=(args.rho_weight,) + CHANNEL_WEIGHTS[1:])
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t1
@@ -457,7 +479,7 @@ def _run(args, stream, out, log):
     err = np.abs(warm["drag"] - rest["drag"]) / np.maximum(np.abs(rest["drag"]), 1e-30)
     res = {
         "train_cases": len(train_seeds), "train_steady": int(sum(r["stable"] and r["steps_to_steady"] > 0 for r in rec)),
-        "epochs": args.epochs, "train_s": round(train_s, 1), "loss_first": hist[0], "loss_last": hist[-1],
+        "epochs": len(hist) if not args.eval_weights else 0, "train_s": round(train_s, 1), "loss_first": hist[0], "loss_last": hist[-1],
         "heldout": len(held), "both_steady": int(ok.sum()),
         "rest_steps_mean": float(rest["steps"][ok].mean()) if ok.any() else None,
         "warm_steps_mean": float(warm["steps"][ok].mean()) if ok.any() else None,
