@@ -389,6 +389,7 @@ def main(argv=None):
     ap.add_argument("--heldout", type=int, default=32)
     ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--group", type=int, default=64, help="cases stepped together in data generation")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--max-steps", type=int, default=40000, help="cap of the data-generation runs")
     ap.add_argument("--eval-max-steps", type=int, default=60000, help="cap of the evaluation runs")
@@ -434,7 +435,7 @@ def _run(args, stream, out, log):
         model = UNet3D.load(args.eval_weights, 0, stream)
         rec, hist, train_s, train_seeds = [], [float("nan")], 0.0, []
     else:
-        X, T, M, counts, rec = generate(train_seeds, 0, stream, args.max_steps, args.tol, log=log,
+        X, T, M, counts, rec = generate(train_seeds, 0, stream, args.max_steps, args.tol, group=args.group, log=log,
                                         augment=args.augment)
         log(f"training set: {X.shape[0]} steady states of {len(train_seeds)} ({time.perf_counter() - t0:.0f} s)")
         epochs = args.epochs
