@@ -1,6 +1,6 @@
 """What the trained network gains: held-out channel cases started from its prediction
 reach steady drag in fewer steps than from rest, at the same drag (weights:
-tests/golden/unet_c5.npz, trained by lbm3d_bb_b200.warmstart on seeds 0..255)."""
+tests/golden/unet_c5.npz, trained by lbm3d_bb_b200.warmstart on seeds 0..2047)."""
 from pathlib import Path
 
 import numpy as np

@@ -48,3 +48,24 @@ def test_mirror_images(fy, fz):
     assert np.array_equal(tt, t)
     m1 = W.mirror_target(t, fy, fz)
     assert m1[0, 0, 0, 2] == (-t[-1 if fz else 0, -1 if fy else 0, 0, 2] if fy else t[-1 if fz else 0, 0, 0, 2])
+
+
+def test_committed_evaluation_record_is_consistent():
+    """The evaluation record of the committed weights (tests/golden/unet_c5_eval.json):
+    its aggregates follow from its per-case steps and drags."""
+    import json
+    from pathlib import Path
+
+    r = json.loads((Path(__file__).resolve().parent / "golden" / "unet_c5_eval.json").read_text())
+    cases = r["per_case"]
+    assert len(cases) == r["heldout"] == 256
+    ok = [c for c in cases if c["rest_steps"] > 0 and c["warm_steps"] > 0]
+    assert len(ok) == r["both_steady"]
+    rest = np.array([c["rest_steps"] for c in ok], float)
+    warm = np.array([c["warm_steps"] for c in ok], float)
+    assert abs(rest.mean() - r["rest_steps_mean"]) < 1e-6 * rest.mean()
+    assert abs(warm.mean() - r["warm_steps_mean"]) < 1e-6 * warm.mean()
+    assert abs(np.mean(rest / warm) - r["step_ratio_mean"]) < 1e-9
+    err = [abs(c["drag_warm"] - c["drag_rest"]) / abs(c["drag_rest"]) for c in ok]
+    assert max(err) <= 5e-3  # the 0.5 % drag contract
+    assert abs(r["wall_speedup"] - r["rest_set_ms"] / r["warm_set_ms"]) < 1e-9
