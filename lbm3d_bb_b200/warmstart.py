@@ -21,8 +21,9 @@ change over 100 steps stays below `drag_tol` for three checks in a row (evaluati
 A warm start computes the first-step residual ||u(1) - u(0)|| / ||u(0)||; above
 `fallback` the case restarts from rest (the plain method remains the fallback).
 
-Usage (one GPU):  python -m lbm3d_bb_b200.warmstart --train 256 --heldout 64 --epochs 200 --out DIR
-                  python -m lbm3d_bb_b200.warmstart --heldout 64 --eval-weights WEIGHTS.npz --out DIR
+Usage (one GPU):  python -m lbm3d_bb_b200.warmstart --train 2048 --heldout 256 --epochs 200 --group 128 \
+                      [--time-budget SECONDS] --out DIR
+                  python -m lbm3d_bb_b200.warmstart --heldout 256 --eval-weights WEIGHTS.npz --out DIR
 """
 from __future__ import annotations
 
