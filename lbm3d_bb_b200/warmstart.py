@@ -283,6 +283,14 @@ def generate(seeds: Sequence[int], device: int = 0, stream=None, max_steps: int 
     return torch.stack(feats), torch.stack(targs), torch.stack(masks), np.array(counts), record
 
 
+def epochs_within(seconds: float, step_s: float, n: int, batch: int, wanted: int) -> int:
+    """Epochs of `n` samples in mini-batches of `batch` that fit `seconds` at `step_s` per
+    training step: at least one, at most `wanted`."""
+    per_epoch = step_s * max(1, n // batch)
+    fit = int(seconds / per_epoch) if per_epoch > 0 else wanted
+    return max(1, min(wanted, fit))
+
+
 def train(model, X, T, M, counts, epochs: int, batch: int = 4, lr: float = 1e-3, seed: int = 0, log=print,
           lr_min: float = 1e-5, weights=CHANNEL_WEIGHTS):
     """Adam on the masked MSE over the GPU-resident data set (shuffled mini-batches
@@ -454,8 +462,7 @@ def _run(args, stream, out, log):
             step_s = (time.perf_counter() - tp) / 8
             del probe
             left = args.time_budget - (time.perf_counter() - t0) - args.eval_reserve
-            fit = int(left / (step_s * max(1, X.shape[0] // args.batch)))
-            epochs = max(1, min(args.epochs, fit))
+            epochs = epochs_within(left, step_s, X.shape[0], args.batch, args.epochs)
             log(f"time budget: {step_s * 1e3:.1f} ms per training step, {left:.0f} s left for training: "
                 f"{epochs} epochs")
         model = UNet3D(16, 0, stream, seed=0)

@@ -69,3 +69,13 @@ def test_committed_evaluation_record_is_consistent():
     err = [abs(c["drag_warm"] - c["drag_rest"]) / abs(c["drag_rest"]) for c in ok]
     assert max(err) <= 5e-3  # the 0.5 % drag contract
     assert abs(r["wall_speedup"] - r["rest_set_ms"] / r["warm_set_ms"]) < 1e-9
+
+
+def test_epochs_fit_the_time_budget():
+    from lbm3d_bb_b200.warmstart import epochs_within
+
+    # 2048 samples, batch 4: 512 steps per epoch at 17.9 ms -> 9.16 s per epoch
+    assert epochs_within(732.0, 0.0179, 2048, 4, 200) == 79
+    assert epochs_within(1e6, 0.0179, 2048, 4, 200) == 200  # capped at the wanted count
+    assert epochs_within(-5.0, 0.0179, 2048, 4, 200) == 1  # at least one epoch
+    assert epochs_within(10.0, 0.0, 2048, 4, 200) == 200
